@@ -1,0 +1,549 @@
+// Neighbour search on sm_100a: periodic cell list with warp-ballot compaction,
+// an all-pairs path for molecules and small boxes, and the skin/cutoff filter.
+//
+// Replaces FeNNol's GraphGenerator.__call__/process/update_skin and
+// GraphFilter (src/fennol/models/preprocessing.py:74-696, 834-960).  The
+// pair predicate reproduces the reference's float32 numpy arithmetic exactly
+// (see common.cuh: no FMA contraction, (x*x+y*y)+z*z, threshold rounded from
+// the double cutoff), so the kept pair set is the reference's.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+
+using namespace fnl;
+
+namespace {
+
+constexpr int kBuildWarps = 4;      // warps per block in the row builders
+constexpr int kMaxSortRow = 1024;   // largest row the in-smem sort handles
+
+struct SysView {
+  const int* start;
+  const int* mode;
+  const float* cell;
+  const float* recip;
+  const int* grid;
+  const int* nrep;
+};
+
+__device__ __forceinline__ size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+struct GraphWs {
+  int* counts;      // [C]
+  int* starts;      // [C+1]
+  int* cursor;      // [C]
+  int* cell_atoms;  // [N]
+  int* atom_cell;   // [N]  (-1: all-pairs system)
+  float4* pos;      // [N]  wrapped (general PBC) or raw positions
+  unsigned* at;     // [N]  packed wrap shift (general PBC)
+};
+
+__host__ size_t ws_layout(int n, int c, char* base, GraphWs* w) {
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t o = off;
+    off = (off + bytes + 255) / 256 * 256;
+    return o;
+  };
+  size_t o_counts = take(sizeof(int) * (size_t)std::max(c, 1));
+  size_t o_starts = take(sizeof(int) * (size_t)(c + 1));
+  size_t o_cursor = take(sizeof(int) * (size_t)std::max(c, 1));
+  size_t o_catoms = take(sizeof(int) * (size_t)std::max(n, 1));
+  size_t o_acell = take(sizeof(int) * (size_t)std::max(n, 1));
+  size_t o_pos = take(sizeof(float4) * (size_t)std::max(n, 1));
+  size_t o_at = take(sizeof(unsigned) * (size_t)std::max(n, 1));
+  if (w && base) {
+    w->counts = (int*)(base + o_counts);
+    w->starts = (int*)(base + o_starts);
+    w->cursor = (int*)(base + o_cursor);
+    w->cell_atoms = (int*)(base + o_catoms);
+    w->atom_cell = (int*)(base + o_acell);
+    w->pos = (float4*)(base + o_pos);
+    w->at = (unsigned*)(base + o_at);
+  }
+  return off;
+}
+
+// ---------------------------------------------------------------------------
+// 1. per atom: arithmetic position (wrapped for general PBC), wrap shift,
+//    cell id and cell histogram.
+// ---------------------------------------------------------------------------
+__global__ void k_prepare(const float* __restrict__ coords, int n, const int* __restrict__ atom_sys,
+                          SysView sv, GraphWs w, const int* enable_flag) {
+  if (enable_flag && *enable_flag == 0) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int b = atom_sys[i];
+  int mode = sv.mode[b];
+  float x = coords[3 * i], y = coords[3 * i + 1], z = coords[3 * i + 2];
+  unsigned at = 0;
+  const float* c = sv.cell + 9 * b;
+  const float* r = sv.recip + 9 * b;
+  if (mode == FENNOL_PBC_GENERAL) {
+    // at_shifts = -floor(x @ recip); x += at_shifts @ cell  (preprocessing.py:144-158)
+    float ax = -floorf(frac_exact(x, y, z, r, 0));
+    float ay = -floorf(frac_exact(x, y, z, r, 1));
+    float az = -floorf(frac_exact(x, y, z, r, 2));
+    add_shift(x, y, z, ax, ay, az, c);
+    at = pack_shift((int)ax, (int)ay, (int)az);
+  }
+  w.pos[i] = make_float4(x, y, z, 0.f);
+  w.at[i] = at;
+  const int* g = sv.grid + 4 * b;
+  if (mode != FENNOL_PBC_NONE && g[0] > 0) {
+    int nc[3] = {g[0], g[1], g[2]};
+    int ci[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      float f = frac_exact(x, y, z, r, d);
+      f -= floorf(f);
+      int k = (int)(f * (float)nc[d]);
+      ci[d] = k < 0 ? 0 : (k >= nc[d] ? nc[d] - 1 : k);
+    }
+    int cell = g[3] + (ci[0] * nc[1] + ci[1]) * nc[2] + ci[2];
+    w.atom_cell[i] = cell;
+    atomicAdd(w.counts + cell, 1);
+  } else {
+    w.atom_cell[i] = -1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 2. exclusive scan of the cell histogram (one block), cursor = start.
+// ---------------------------------------------------------------------------
+__global__ void k_scan(GraphWs w, int c, const int* enable_flag) {
+  if (enable_flag && *enable_flag == 0) return;
+  __shared__ int warp_sums[32];
+  __shared__ int carry;
+  int tid = threadIdx.x;
+  if (tid == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < c; base += blockDim.x) {
+    int idx = base + tid;
+    int v = idx < c ? w.counts[idx] : 0;
+    int lane = tid & 31, wid = tid >> 5;
+    int incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) warp_sums[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+      int nw = blockDim.x >> 5;
+      int s = lane < nw ? warp_sums[lane] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, s, o);
+        if (lane >= o) s += t;
+      }
+      if (lane < nw) warp_sums[lane] = s;
+    }
+    __syncthreads();
+    int excl = carry + (wid > 0 ? warp_sums[wid - 1] : 0) + incl - v;
+    if (idx < c) {
+      w.starts[idx] = excl;
+      w.cursor[idx] = excl;
+    }
+    __syncthreads();
+    if (tid == blockDim.x - 1) carry = excl + v;
+    __syncthreads();
+  }
+  if (tid == 0) w.starts[c] = carry;
+}
+
+// 3. scatter atoms into their cells (order inside a cell is arbitrary; rows are
+//    sorted afterwards so the final lists are deterministic).
+__global__ void k_scatter(int n, GraphWs w, const int* enable_flag) {
+  if (enable_flag && *enable_flag == 0) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int cell = w.atom_cell[i];
+  if (cell < 0) return;
+  int slot = atomicAdd(w.cursor + cell, 1);
+  w.cell_atoms[slot] = i;
+}
+
+// Candidate test for the pair (i, j) with image shift `img` (general PBC) or
+// the rounding shift (minimum image); returns true and the stored shift when
+// d^2 < rc2.
+__device__ __forceinline__ bool pair_test(int mode, float4 pi, float4 pj, unsigned ati, unsigned atj,
+                                          int ix, int iy, int iz, const float* c, const float* r,
+                                          float rc2, unsigned& shift_out) {
+  float vx = __fsub_rn(pj.x, pi.x), vy = __fsub_rn(pj.y, pi.y), vz = __fsub_rn(pj.z, pi.z);
+  int sx = 0, sy = 0, sz = 0;
+  if (mode == FENNOL_PBC_MINIMUM_IMAGE) {
+    // pbc_shifts = -round(vec @ recip); vec += pbc_shifts @ cell (preprocessing.py:127-143)
+    float fx = -rintf(frac_exact(vx, vy, vz, r, 0));
+    float fy = -rintf(frac_exact(vx, vy, vz, r, 1));
+    float fz = -rintf(frac_exact(vx, vy, vz, r, 2));
+    add_shift(vx, vy, vz, fx, fy, fz, c);
+    sx = (int)fx;
+    sy = (int)fy;
+    sz = (int)fz;
+  } else if (mode == FENNOL_PBC_GENERAL) {
+    if (ix | iy | iz) add_shift(vx, vy, vz, (float)ix, (float)iy, (float)iz, c);
+    int ax, ay, az, bx, by, bz;
+    unpack_shift(ati, ax, ay, az);
+    unpack_shift(atj, bx, by, bz);
+    sx = ix + bx - ax;
+    sy = iy + by - ay;
+    sz = iz + bz - az;
+  }
+  float d2 = dist2_exact(vx, vy, vz);
+  shift_out = pack_shift(sx, sy, sz);
+  return d2 < rc2;
+}
+
+// Bitonic sort of `m` (power of two) 64-bit keys in shared memory by one warp.
+__device__ void warp_bitonic_sort(unsigned long long* keys, int m, int lane) {
+  for (int k = 2; k <= m; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int idx = lane; idx < m; idx += 32) {
+        int ixj = idx ^ j;
+        if (ixj > idx) {
+          unsigned long long a = keys[idx], b = keys[ixj];
+          bool up = (idx & k) == 0;
+          if ((a > b) == up) {
+            keys[idx] = b;
+            keys[ixj] = a;
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+__device__ __forceinline__ unsigned long long make_key(int j, unsigned shift) {
+  return ((unsigned long long)(unsigned)j << 32) | (unsigned long long)shift;
+}
+
+// Append candidates selected by `keep` (one per lane) to the warp's key row.
+__device__ __forceinline__ void warp_append(bool keep, int j, unsigned shift, unsigned long long* keys,
+                                            int cap, int& count, int lane) {
+  unsigned m = __ballot_sync(0xffffffffu, keep);
+  if (keep) {
+    int pos = count + warp_exclusive_prefix(m, lane);
+    if (pos < cap) keys[pos] = make_key(j, shift);
+  }
+  count += __popc(m);
+}
+
+__device__ void finish_row(int i, unsigned long long* keys, int count, int cap, int sort_len,
+                           int* __restrict__ nbr_j, unsigned* __restrict__ nbr_shift,
+                           int* __restrict__ nbr_count, int* status, int lane) {
+  int stored = count < cap ? count : cap;
+  if (count > cap) {
+    if (lane == 0) {
+      status_set(status, ST_NBR_OVERFLOW);
+    }
+  }
+  if (lane == 0) status_max(status, ST_NBR_MAXCOUNT, count);
+  // pad and sort the stored part
+  int m = 1;
+  while (m < stored) m <<= 1;
+  if (m > sort_len) m = sort_len;
+  for (int k = stored + lane; k < m; k += 32) keys[k] = ~0ull;
+  __syncwarp();
+  if (stored > 1) warp_bitonic_sort(keys, m, lane);
+  size_t base = (size_t)i * cap;
+  for (int k = lane; k < stored; k += 32) {
+    unsigned long long key = keys[k];
+    nbr_j[base + k] = (int)(key >> 32);
+    nbr_shift[base + k] = (unsigned)(key & 0xFFFFFFFFull);
+  }
+  if (lane == 0) nbr_count[i] = stored;
+  __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
+// 4a. cell-list rows: one warp per atom, 27 stencil cells, ballot compaction.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBuildWarps * 32)
+k_build_cells(int n, const int* __restrict__ atom_sys, SysView sv, GraphWs w, float rc2, int cap,
+              int sort_len, int* __restrict__ nbr_j, unsigned* __restrict__ nbr_shift,
+              int* __restrict__ nbr_count, int* status, const int* enable_flag) {
+  if (enable_flag && *enable_flag == 0) return;
+  extern __shared__ unsigned long long smem_keys[];
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int i = blockIdx.x * kBuildWarps + warp;
+  if (i >= n) return;
+  int cell = w.atom_cell[i];
+  if (cell < 0) return;  // all-pairs system
+  unsigned long long* keys = smem_keys + (size_t)warp * sort_len;
+  int b = atom_sys[i];
+  int mode = sv.mode[b];
+  const float* c = sv.cell + 9 * b;
+  const float* r = sv.recip + 9 * b;
+  const int* g = sv.grid + 4 * b;
+  int nx = g[0], ny = g[1], nz = g[2], off = g[3];
+  int local = cell - off;
+  int cz = local % nz, cy = (local / nz) % ny, cx = local / (ny * nz);
+  float4 pi = w.pos[i];
+  unsigned ati = w.at[i];
+  int count = 0;
+  for (int dx = -1; dx <= 1; ++dx) {
+    int ex = cx + dx, wx = 0;
+    if (ex < 0) { ex += nx; wx = -1; } else if (ex >= nx) { ex -= nx; wx = 1; }
+    for (int dy = -1; dy <= 1; ++dy) {
+      int ey = cy + dy, wy = 0;
+      if (ey < 0) { ey += ny; wy = -1; } else if (ey >= ny) { ey -= ny; wy = 1; }
+      for (int dz = -1; dz <= 1; ++dz) {
+        int ez = cz + dz, wz = 0;
+        if (ez < 0) { ez += nz; wz = -1; } else if (ez >= nz) { ez -= nz; wz = 1; }
+        int nc = off + (ex * ny + ey) * nz + ez;
+        int s0 = w.starts[nc], s1 = w.starts[nc + 1];
+        for (int k0 = s0; k0 < s1; k0 += 32) {
+          int k = k0 + lane;
+          bool keep = false;
+          int j = -1;
+          unsigned sh = 0;
+          if (k < s1) {
+            j = w.cell_atoms[k];
+            if (j != i)
+              keep = pair_test(mode, pi, w.pos[j], ati, w.at[j], wx, wy, wz, c, r, rc2, sh);
+          }
+          warp_append(keep, j, sh, keys, cap, count, lane);
+        }
+      }
+    }
+  }
+  __syncwarp();
+  finish_row(i, keys, count, cap, sort_len, nbr_j, nbr_shift, nbr_count, status, lane);
+}
+
+// ---------------------------------------------------------------------------
+// 4b. all-pairs rows (molecules, boxes too small for a 3x3x3 cell stencil).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBuildWarps * 32)
+k_build_allpairs(int n, const int* __restrict__ atom_sys, SysView sv, GraphWs w, float rc2, int cap,
+                 int sort_len, int* __restrict__ nbr_j, unsigned* __restrict__ nbr_shift,
+                 int* __restrict__ nbr_count, int* status, const int* enable_flag) {
+  if (enable_flag && *enable_flag == 0) return;
+  extern __shared__ unsigned long long smem_keys[];
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int i = blockIdx.x * kBuildWarps + warp;
+  if (i >= n) return;
+  if (w.atom_cell[i] >= 0) return;  // cell-list system
+  unsigned long long* keys = smem_keys + (size_t)warp * sort_len;
+  int b = atom_sys[i];
+  int mode = sv.mode[b];
+  const float* c = sv.cell + 9 * b;
+  const float* r = sv.recip + 9 * b;
+  int j0 = sv.start[b], j1 = sv.start[b + 1];
+  int rx = 0, ry = 0, rz = 0;
+  if (mode == FENNOL_PBC_GENERAL) {
+    rx = sv.nrep[3 * b];
+    ry = sv.nrep[3 * b + 1];
+    rz = sv.nrep[3 * b + 2];
+  }
+  float4 pi = w.pos[i];
+  unsigned ati = w.at[i];
+  int count = 0;
+  for (int ix = -rx; ix <= rx; ++ix)
+    for (int iy = -ry; iy <= ry; ++iy)
+      for (int iz = -rz; iz <= rz; ++iz) {
+        for (int k0 = j0; k0 < j1; k0 += 32) {
+          int j = k0 + lane;
+          bool keep = false;
+          unsigned sh = 0;
+          if (j < j1 && j != i)
+            keep = pair_test(mode, pi, w.pos[j], ati, w.at[j], ix, iy, iz, c, r, rc2, sh);
+          warp_append(keep, j, sh, keys, cap, count, lane);
+        }
+      }
+  __syncwarp();
+  finish_row(i, keys, count, cap, sort_len, nbr_j, nbr_shift, nbr_count, status, lane);
+}
+
+__global__ void k_count_rebuild(int* status, const int* enable_flag) {
+  if (enable_flag && *enable_flag == 0) return;
+  if (status) atomicAdd(status + ST_REBUILD_COUNT, 1);
+}
+
+// ---------------------------------------------------------------------------
+// Filter a list to a smaller cutoff (update_skin / GraphFilter).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+k_filter(const float* __restrict__ coords, int n, const int* __restrict__ atom_sys,
+         const float* __restrict__ sys_cell, const int* __restrict__ in_j,
+         const unsigned* __restrict__ in_shift, const int* __restrict__ in_count, int in_cap,
+         float rc2, int out_cap, int* __restrict__ out_j, unsigned* __restrict__ out_shift,
+         int* __restrict__ out_count, int* status) {
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  int i = warp;
+  int b = atom_sys[i];
+  const float* c = sys_cell ? sys_cell + 9 * b : nullptr;
+  float xi = coords[3 * i], yi = coords[3 * i + 1], zi = coords[3 * i + 2];
+  int cnt = in_count[i];
+  if (cnt > in_cap) cnt = in_cap;
+  size_t ib = (size_t)i * in_cap, ob = (size_t)i * out_cap;
+  int count = 0;
+  for (int k0 = 0; k0 < cnt; k0 += 32) {
+    int k = k0 + lane;
+    bool keep = false;
+    int j = 0;
+    unsigned sh = 0;
+    if (k < cnt) {
+      j = in_j[ib + k];
+      sh = in_shift[ib + k];
+      float vx = __fsub_rn(coords[3 * j], xi);
+      float vy = __fsub_rn(coords[3 * j + 1], yi);
+      float vz = __fsub_rn(coords[3 * j + 2], zi);
+      if (sh && c) {
+        int sx, sy, sz;
+        unpack_shift(sh, sx, sy, sz);
+        add_shift(vx, vy, vz, (float)sx, (float)sy, (float)sz, c);
+      }
+      keep = dist2_exact(vx, vy, vz) < rc2;
+    }
+    unsigned m = __ballot_sync(0xffffffffu, keep);
+    if (keep) {
+      int pos = count + warp_exclusive_prefix(m, lane);
+      if (pos < out_cap) {
+        out_j[ob + pos] = j;
+        out_shift[ob + pos] = sh;
+      }
+    }
+    count += __popc(m);
+  }
+  if (lane == 0) {
+    out_count[i] = count < out_cap ? count : out_cap;
+    if (count > out_cap) status_set(status, ST_FILTER_OVERFLOW);
+    status_max(status, ST_FILTER_MAXCOUNT, count);
+  }
+}
+
+}  // namespace
+
+extern "C" int fennol_graph_plan(int nsys, const int* host_mode, const float* host_recip,
+                                 double cutoff, int* host_grid, int* host_nrep) {
+  if (nsys < 0 || !host_mode || !host_grid || !host_nrep || !(cutoff > 0)) return FENNOL_ERR_INVALID;
+  long long total = 0;
+  for (int b = 0; b < nsys; ++b) {
+    int* g = host_grid + 4 * b;
+    int* nr = host_nrep + 3 * b;
+    g[0] = g[1] = g[2] = 0;
+    g[3] = (int)total;
+    nr[0] = nr[1] = nr[2] = 0;
+    if (host_mode[b] == FENNOL_PBC_NONE) continue;
+    if (!host_recip) return FENNOL_ERR_INVALID;
+    const float* r = host_recip + 9 * b;
+    int nc[3];
+    bool ok = true;
+    for (int d = 0; d < 3; ++d) {
+      // |recip column d| as in preprocessing.py:161-163 (float32)
+      float s = 0.f;
+      for (int k = 0; k < 3; ++k) s += r[3 * k + d] * r[3 * k + d];
+      float inv = sqrtf(s);
+      nr[d] = (int)std::ceil((float)cutoff * inv);
+      // bins wider than the cutoff by a relative margin (binning round-off)
+      double width = 1.0 / ((double)inv * cutoff * (1.0 + 1e-5));
+      long long k = (long long)std::floor(width);
+      if (k > 256) k = 256;
+      nc[d] = (int)k;
+      if (k < 3) ok = false;
+    }
+    if (ok) {
+      g[0] = nc[0];
+      g[1] = nc[1];
+      g[2] = nc[2];
+      total += (long long)nc[0] * nc[1] * nc[2];
+      if (total > (1ll << 30)) return FENNOL_ERR_UNSUPPORTED;
+    }
+  }
+  return (int)total;
+}
+
+extern "C" size_t fennol_graph_workspace_bytes(int natoms, int ncells_total) {
+  if (natoms < 0 || ncells_total < 0) return 0;
+  return ws_layout(natoms, ncells_total, nullptr, nullptr);
+}
+
+static int sort_len_for(int cap) {
+  int m = 1;
+  while (m < cap) m <<= 1;
+  return m;
+}
+
+extern "C" int fennol_graph_build(const float* coords, int natoms, const int* atom_sys, int nsys,
+                                  const int* sys_start, const int* sys_mode, const float* sys_cell,
+                                  const float* sys_recip, const int* sys_grid, const int* sys_nrep,
+                                  int ncells_total, double cutoff, int capacity, int* nbr_j,
+                                  unsigned* nbr_shift, int* nbr_count, int* status, void* workspace,
+                                  size_t workspace_bytes, const int* enable_flag, void* stream) {
+  if (natoms < 0 || nsys <= 0 || capacity <= 0 || capacity > kMaxSortRow || !(cutoff > 0))
+    return FENNOL_ERR_INVALID;
+  if (natoms == 0) return FENNOL_OK;
+  if (!coords || !atom_sys || !sys_start || !sys_mode || !sys_grid || !sys_nrep || !nbr_j ||
+      !nbr_shift || !nbr_count || !workspace || !sys_cell || !sys_recip)
+    return FENNOL_ERR_INVALID;
+  if (workspace_bytes < fennol_graph_workspace_bytes(natoms, ncells_total)) return FENNOL_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  GraphWs w;
+  ws_layout(natoms, ncells_total, (char*)workspace, &w);
+  SysView sv{sys_start, sys_mode, sys_cell, sys_recip, sys_grid, sys_nrep};
+  float rc2 = (float)(cutoff * cutoff);
+  int sort_len = sort_len_for(capacity);
+  size_t smem = (size_t)kBuildWarps * sort_len * sizeof(unsigned long long);
+  if (smem > 48 * 1024) {
+    if (cudaFuncSetAttribute(k_build_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_build_allpairs, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
+      return FENNOL_ERR_CUDA;
+  }
+  if (ncells_total > 0) {
+    if (cudaMemsetAsync(w.counts, 0, sizeof(int) * (size_t)ncells_total, st) != cudaSuccess)
+      return FENNOL_ERR_CUDA;
+  }
+  int tb = 256;
+  int gb = (natoms + tb - 1) / tb;
+  k_prepare<<<gb, tb, 0, st>>>(coords, natoms, atom_sys, sv, w, enable_flag);
+  FNL_CHECK_LAUNCH();
+  if (ncells_total > 0) {
+    k_scan<<<1, 1024, 0, st>>>(w, ncells_total, enable_flag);
+    FNL_CHECK_LAUNCH();
+    k_scatter<<<gb, tb, 0, st>>>(natoms, w, enable_flag);
+    FNL_CHECK_LAUNCH();
+  }
+  int gw = (natoms + kBuildWarps - 1) / kBuildWarps;
+  if (ncells_total > 0) {
+    k_build_cells<<<gw, kBuildWarps * 32, smem, st>>>(natoms, atom_sys, sv, w, rc2, capacity, sort_len,
+                                                       nbr_j, nbr_shift, nbr_count, status, enable_flag);
+    FNL_CHECK_LAUNCH();
+  }
+  k_build_allpairs<<<gw, kBuildWarps * 32, smem, st>>>(natoms, atom_sys, sv, w, rc2, capacity, sort_len,
+                                                        nbr_j, nbr_shift, nbr_count, status, enable_flag);
+  FNL_CHECK_LAUNCH();
+  if (status) {
+    k_count_rebuild<<<1, 1, 0, st>>>(status, enable_flag);
+    FNL_CHECK_LAUNCH();
+  }
+  return FENNOL_OK;
+}
+
+extern "C" int fennol_graph_filter(const float* coords, int natoms, const int* atom_sys,
+                                   const float* sys_cell, const int* in_j, const unsigned* in_shift,
+                                   const int* in_count, int in_capacity, double cutoff,
+                                   int out_capacity, int* out_j, unsigned* out_shift, int* out_count,
+                                   int* status, void* stream) {
+  if (natoms < 0 || in_capacity <= 0 || out_capacity <= 0 || !(cutoff > 0)) return FENNOL_ERR_INVALID;
+  if (natoms == 0) return FENNOL_OK;
+  if (!coords || !atom_sys || !in_j || !in_shift || !in_count || !out_j || !out_shift || !out_count)
+    return FENNOL_ERR_INVALID;
+  float rc2 = (float)(cutoff * cutoff);
+  int threads = 256;
+  long long blocks = ((long long)natoms * 32 + threads - 1) / threads;
+  k_filter<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
+      coords, natoms, atom_sys, sys_cell, in_j, in_shift, in_count, in_capacity, rc2, out_capacity,
+      out_j, out_shift, out_count, status);
+  FNL_CHECK_LAUNCH();
+  return FENNOL_OK;
+}

@@ -1,0 +1,217 @@
+// Energy reduction, force output and the float64 MD integrator step.
+//
+// fennol_energy_reduce replaces the per-system segment_sum of
+// FENNIX.total_energy (src/fennol/models/fennix.py:218-258) with a float64,
+// fixed-order reduction.  fennol_md_step is the integrate() step of
+// src/fennol/md/integrate.py:286-294 with the Langevin O step of
+// src/fennol/md/thermostats.py:56-120 (NVE, :172-190, when a2 is NULL),
+// carried in float64 and kept on the device.
+#include <cmath>
+
+#include "common.cuh"
+
+using namespace fnl;
+
+namespace {
+
+__global__ void k_energy_reduce(const float* __restrict__ e_rows, const int* __restrict__ atom_row,
+                                const int* __restrict__ sys_start, double scale,
+                                double* __restrict__ energy, double* __restrict__ e_atom) {
+  __shared__ double part[256];
+  int b = blockIdx.x;
+  int i0 = sys_start[b], i1 = sys_start[b + 1];
+  double s = 0.0;
+  for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+    double e = scale * (double)e_rows[atom_row[i]];
+    if (e_atom) e_atom[i] = e;
+    s += e;
+  }
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) energy[b] = part[0];
+}
+
+__global__ void k_forces_finalize(const float4* __restrict__ f4, int n, float scale, float* __restrict__ f) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 v = f4[i];
+  f[3 * i] = scale * v.x;
+  f[3 * i + 1] = scale * v.y;
+  f[3 * i + 2] = scale * v.z;
+}
+
+// Philox4x32-10 counter-based generator (Salmon, Moraes, Dror, Shaw, SC'11).
+struct U4 {
+  unsigned x, y, z, w;
+};
+__device__ __forceinline__ U4 philox4x32_10(U4 c, unsigned k0, unsigned k1) {
+  const unsigned M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+  const unsigned W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    unsigned hi0 = __umulhi(M0, c.x), lo0 = M0 * c.x;
+    unsigned hi1 = __umulhi(M1, c.z), lo1 = M1 * c.z;
+    c = U4{hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0};
+    k0 += W0;
+    k1 += W1;
+  }
+  return c;
+}
+
+// Box-Muller on two 32-bit uniforms -> two standard normals (float64).
+__device__ __forceinline__ void box_muller(unsigned a, unsigned b, double& z0, double& z1) {
+  double u1 = ((double)a + 1.0) * (1.0 / 4294967296.0);  // (0, 1]
+  double u2 = (double)b * (1.0 / 4294967296.0);          // [0, 1)
+  double r = sqrt(-2.0 * log(u1));
+  double s, c;
+  sincospi(2.0 * u2, &s, &c);
+  z0 = r * c;
+  z1 = r * s;
+}
+
+__global__ void k_md_step(int n, double dt, double* __restrict__ x, double* __restrict__ v,
+                          const double* __restrict__ inv_mass, const float4* __restrict__ f4,
+                          double fscale, double a1, const double* __restrict__ a2,
+                          unsigned long long seed, unsigned long long step, float* __restrict__ coords,
+                          const int* __restrict__ sp, float4* __restrict__ xyzs,
+                          const double* __restrict__ x_ref, double half_skin2, int* rebuild_flag) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 f = f4[i];
+  double im = inv_mass[i];
+  double vx = v[3 * i], vy = v[3 * i + 1], vz = v[3 * i + 2];
+  double px = x[3 * i], py = x[3 * i + 1], pz = x[3 * i + 2];
+  // B: v += dt/m F
+  vx += dt * im * (fscale * (double)f.x);
+  vy += dt * im * (fscale * (double)f.y);
+  vz += dt * im * (fscale * (double)f.z);
+  // A: x += dt/2 v
+  double h = 0.5 * dt;
+  px += h * vx;
+  py += h * vy;
+  pz += h * vz;
+  // O: Langevin
+  if (a2) {
+    U4 r = philox4x32_10(U4{(unsigned)i, (unsigned)(step & 0xffffffffull), (unsigned)(step >> 32), 0x4C47u},
+                         (unsigned)(seed & 0xffffffffull), (unsigned)(seed >> 32));
+    double z0, z1, z2, z3;
+    box_muller(r.x, r.y, z0, z1);
+    box_muller(r.z, r.w, z2, z3);
+    double s = a2[i];
+    vx = a1 * vx + s * z0;
+    vy = a1 * vy + s * z1;
+    vz = a1 * vz + s * z2;
+  }
+  // A: x += dt/2 v
+  px += h * vx;
+  py += h * vy;
+  pz += h * vz;
+  v[3 * i] = vx;
+  v[3 * i + 1] = vy;
+  v[3 * i + 2] = vz;
+  x[3 * i] = px;
+  x[3 * i + 1] = py;
+  x[3 * i + 2] = pz;
+  float fx = (float)px, fy = (float)py, fz = (float)pz;
+  if (coords) {
+    coords[3 * i] = fx;
+    coords[3 * i + 1] = fy;
+    coords[3 * i + 2] = fz;
+  }
+  if (xyzs) xyzs[i] = make_float4(fx, fy, fz, __int_as_float(sp[i]));
+  if (rebuild_flag && x_ref) {
+    double dx = px - x_ref[3 * i], dy = py - x_ref[3 * i + 1], dz = pz - x_ref[3 * i + 2];
+    if (dx * dx + dy * dy + dz * dz > half_skin2) *rebuild_flag = 1;
+  }
+}
+
+__global__ void k_mark_rebuilt(int n, const double* __restrict__ x, double* __restrict__ x_ref, int* flag) {
+  if (*flag == 0) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < 3 * n) x_ref[i] = x[i];
+}
+__global__ void k_clear_flag(int* flag) { *flag = 0; }
+
+__global__ void k_kinetic(int n, const double* __restrict__ v, const double* __restrict__ inv_mass,
+                          double* out) {
+  __shared__ double part[1024];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double vx = v[3 * i], vy = v[3 * i + 1], vz = v[3 * i + 2];
+    s += (vx * vx + vy * vy + vz * vz) / inv_mass[i];
+  }
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = 0.5 * part[0];
+}
+
+}  // namespace
+
+extern "C" int fennol_energy_reduce(const float* e_rows, const int* atom_row, int natoms,
+                                    const int* sys_start, int nsys, double scale, double* energy,
+                                    double* e_atom, void* stream) {
+  if (natoms < 0 || nsys < 0) return FENNOL_ERR_INVALID;
+  if (nsys == 0) return FENNOL_OK;
+  if (!e_rows || !atom_row || !sys_start || !energy) return FENNOL_ERR_INVALID;
+  k_energy_reduce<<<nsys, 256, 0, (cudaStream_t)stream>>>(e_rows, atom_row, sys_start, scale, energy,
+                                                          e_atom);
+  FNL_CHECK_LAUNCH();
+  return FENNOL_OK;
+}
+
+extern "C" int fennol_forces_finalize(const float* forces4, int natoms, float scale, float* forces,
+                                      void* stream) {
+  if (natoms < 0) return FENNOL_ERR_INVALID;
+  if (natoms == 0) return FENNOL_OK;
+  if (!forces4 || !forces) return FENNOL_ERR_INVALID;
+  k_forces_finalize<<<(natoms + 255) / 256, 256, 0, (cudaStream_t)stream>>>((const float4*)forces4, natoms,
+                                                                             scale, forces);
+  FNL_CHECK_LAUNCH();
+  return FENNOL_OK;
+}
+
+extern "C" int fennol_md_step(int natoms, double dt, double* x, double* v, const double* inv_mass,
+                              const float* forces4, double force_scale, double a1, const double* a2,
+                              unsigned long long seed, unsigned long long step, float* coords,
+                              const int* species_idx, float* xyzs, const double* x_ref,
+                              double half_skin, int* rebuild_flag, void* stream) {
+  if (natoms < 0 || !(dt > 0)) return FENNOL_ERR_INVALID;
+  if (natoms == 0) return FENNOL_OK;
+  if (!x || !v || !inv_mass || !forces4) return FENNOL_ERR_INVALID;
+  if (xyzs && !species_idx) return FENNOL_ERR_INVALID;
+  k_md_step<<<(natoms + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
+      natoms, dt, x, v, inv_mass, (const float4*)forces4, force_scale, a1, a2, seed, step, coords,
+      species_idx, (float4*)xyzs, x_ref, half_skin * half_skin, rebuild_flag);
+  FNL_CHECK_LAUNCH();
+  return FENNOL_OK;
+}
+
+extern "C" int fennol_md_mark_rebuilt(int natoms, const double* x, double* x_ref, int* rebuild_flag,
+                                      void* stream) {
+  if (natoms < 0 || !x || !x_ref || !rebuild_flag) return FENNOL_ERR_INVALID;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (natoms > 0) {
+    k_mark_rebuilt<<<(3 * natoms + 255) / 256, 256, 0, st>>>(natoms, x, x_ref, rebuild_flag);
+    FNL_CHECK_LAUNCH();
+  }
+  k_clear_flag<<<1, 1, 0, st>>>(rebuild_flag);
+  FNL_CHECK_LAUNCH();
+  return FENNOL_OK;
+}
+
+extern "C" int fennol_md_kinetic(int natoms, const double* v, const double* inv_mass, double* kinetic,
+                                 void* stream) {
+  if (natoms < 0 || !kinetic) return FENNOL_ERR_INVALID;
+  if (natoms > 0 && (!v || !inv_mass)) return FENNOL_ERR_INVALID;
+  k_kinetic<<<1, 1024, 0, (cudaStream_t)stream>>>(natoms, v, inv_mass, kinetic);
+  FNL_CHECK_LAUNCH();
+  return FENNOL_OK;
+}

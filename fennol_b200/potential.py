@@ -1,0 +1,481 @@
+"""Host side of the energy/force path: batch layout, device buffers, launches.
+
+:class:`ANIPotential` owns the packed weights of an (ensemble of) ANI-2x-style
+species networks and evaluates energies and forces of batches of systems
+through the C ABI.  It reproduces what FeNNol does for the same model
+(``FENNIX._energy_and_forces``, ``src/fennol/models/fennix.py:260-272``): the
+GRAPH / GRAPH_FILTER / GRAPH_ANGULAR_EXTENSION / SPECIES_INDEXER preprocessing
+(``preprocessing.py``), ``ANIAEV`` (``embeddings/ani.py``) and
+``SpeciesIndexNet`` (``misc/nets.py``), the energy sum and ``-dE/dx``.
+
+Capacity handling follows the reference's overflow protocol
+(``check_reallocate``, ``preprocessing.py:357-367``): kernels report overflow
+through device status words, the host regrows with a margin
+(``mult_size`` 1.05 + ``add_neigh``) and relaunches.
+"""
+
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import call
+from .params import AEVConfig, MLPConfig, Weights, init_weights
+
+HARTREE_TO_KCALMOL = 627.5096080305927
+TILE = 128
+
+
+def _ceil(a: int, b: int) -> int:
+    return (a + b - 1) // b * b
+
+
+def _ptr(t: Optional[torch.Tensor]) -> Optional[int]:
+    return None if t is None else t.data_ptr()
+
+
+def _stream(device) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def round_weights_bf16(weights: Weights) -> Weights:
+    """Round every kernel to the nearest bfloat16 (biases kept)."""
+    out = []
+    for model in weights:
+        m = {}
+        for sym, layers in model.items():
+            m[sym] = [(torch.tensor(w).to(torch.bfloat16).to(torch.float64).numpy(), b)
+                      for (w, b) in layers]
+        out.append(m)
+    return out
+
+
+class PackedMLP:
+    """Device copies of the species networks in the layouts the kernels read
+    (see ``fennol_mlp_weights`` in ``include/fennol_b200.h``)."""
+
+    def __init__(self, weights: Weights, aev: AEVConfig, mlp: MLPConfig, device, precision: int):
+        self.n_models = len(weights)
+        self.n_species = aev.num_species
+        real = [aev.aev_length, *mlp.hidden, mlp.output_dim]
+        if mlp.output_dim != 1:
+            raise ValueError("the energy network must have one output")
+        dims = [_ceil(d, 64) for d in real[:-1]] + [1]
+        self.real_dims, self.dims = real, dims
+        G = self.n_models * self.n_species
+        w32, b32, wt_hi, wt_lo, w_hi, w_lo = [], [], [], [], [], []
+        for l in range(4):
+            W = np.zeros((G, dims[l], dims[l + 1]))
+            B = np.zeros((G, dims[l + 1]))
+            for m, model in enumerate(weights):
+                for s, sym in enumerate(aev.species_order):
+                    k, b = model[sym][l]
+                    if k.shape != (real[l], real[l + 1]):
+                        raise ValueError(f"layer {l + 1} of {sym}: shape {k.shape}, expected "
+                                         f"{(real[l], real[l + 1])}")
+                    W[m * self.n_species + s, :real[l], :real[l + 1]] = k
+                    B[m * self.n_species + s, :real[l + 1]] = b
+            Wt = torch.tensor(W, dtype=torch.float64)
+            w32.append(Wt.to(torch.float32).to(device).contiguous())
+            b32.append(torch.tensor(B, dtype=torch.float32, device=device).contiguous())
+            if precision != _lib.MLP_FP32 and l < 3:
+                hi = Wt.to(torch.bfloat16)
+                lo = (Wt - hi.to(torch.float64)).to(torch.bfloat16)
+                w_hi.append(hi.to(device).contiguous())
+                w_lo.append(lo.to(device).contiguous())
+                wt_hi.append(hi.transpose(1, 2).contiguous().to(device))
+                wt_lo.append(lo.transpose(1, 2).contiguous().to(device))
+            else:
+                w_hi.append(None), w_lo.append(None), wt_hi.append(None), wt_lo.append(None)
+        self._keep = (w32, b32, wt_hi, wt_lo, w_hi, w_lo)
+        s = _lib.MLPWeights()
+        s.n_models = self.n_models
+        s.n_species = self.n_species
+        for k in range(5):
+            s.dims[k] = dims[k]
+        s.celu_alpha = mlp.celu_alpha
+        for l in range(4):
+            s.w32[l] = _ptr(w32[l])
+            s.b32[l] = _ptr(b32[l])
+            s.wt_hi[l] = _ptr(wt_hi[l])
+            s.wt_lo[l] = _ptr(wt_lo[l])
+            s.w_hi[l] = _ptr(w_hi[l])
+            s.w_lo[l] = _ptr(w_lo[l])
+        self.struct = s
+
+
+def aev_params(cfg: AEVConfig) -> _lib.AEVParams:
+    p = _lib.AEVParams()
+    p.num_species = cfg.num_species
+    p.radial_divisions = cfg.radial_dist_divisions
+    p.angular_divisions = cfg.angular_dist_divisions
+    p.angle_sections = cfg.angle_sections
+    p.radial_cutoff = cfg.radial_cutoff
+    p.angular_cutoff = cfg.angular_cutoff
+    p.radial_eta = cfg.radial_eta
+    p.angular_eta = cfg.angular_eta
+    p.zeta = cfg.zeta
+    p.radial_start = cfg.radial_start
+    p.angular_start = cfg.angular_start
+    return p
+
+
+@dataclasses.dataclass
+class Capacities:
+    """Row lengths of the neighbour lists (reference state keys ``npairs``,
+    ``npairs_skin``, ``max_neigh``)."""
+
+    skin: int = 0
+    radial: int = 0
+
+
+class BatchLayout:
+    """Static description of a batch: systems, cells, species-sorted rows."""
+
+    def __init__(self, species_idx: np.ndarray, natoms: Sequence[int], cells=None,
+                 minimum_image: bool = True, device="cuda"):
+        species_idx = np.asarray(species_idx, dtype=np.int32)
+        natoms = np.asarray(natoms, dtype=np.int64).reshape(-1)
+        n = int(natoms.sum())
+        if species_idx.shape[0] != n:
+            raise ValueError("species and natoms disagree")
+        B = natoms.shape[0]
+        self.natoms = natoms
+        self.n = n
+        self.nsys = B
+        self.device = torch.device(device)
+        start = np.concatenate([[0], np.cumsum(natoms)]).astype(np.int32)
+        self.sys_start_host = start
+        atom_sys = np.repeat(np.arange(B, dtype=np.int32), natoms)
+        cell_arr = np.zeros((B, 3, 3), np.float32)
+        recip_arr = np.zeros((B, 3, 3), np.float32)
+        mode = np.zeros(B, np.int32)
+        if cells is not None:
+            cl = cells if isinstance(cells, (list, tuple)) else list(np.asarray(cells).reshape(-1, 3, 3))
+            if len(cl) == 1 and B > 1:
+                cl = cl * B
+            for b, c in enumerate(cl):
+                if c is None:
+                    continue
+                c32 = np.asarray(c, dtype=np.float32).reshape(3, 3)
+                cell_arr[b] = c32
+                recip_arr[b] = np.linalg.inv(c32).astype(np.float32)
+                mode[b] = _lib.PBC_MINIMUM_IMAGE if minimum_image else _lib.PBC_GENERAL
+        self.has_pbc = bool((mode != 0).any())
+        self.mode_host, self.cell_host, self.recip_host = mode, cell_arr, recip_arr
+        # species-sorted rows, segments padded to the 128-row tile
+        self.species_idx = species_idx
+        S = int(species_idx.max()) + 1 if n else 1
+        row = np.zeros(n, np.int32)
+        tiles_s, tiles_r = [], []
+        off = 0
+        for s in range(max(S, 1)):
+            idx = np.nonzero(species_idx == s)[0]
+            if idx.size == 0:
+                continue
+            row[idx] = off + np.arange(idx.size)
+            for t in range((idx.size + TILE - 1) // TILE):
+                tiles_s.append(s)
+                tiles_r.append(off + t * TILE)
+            off += _ceil(idx.size, TILE)
+        self.rows = max(off, TILE)
+        self.ntiles = len(tiles_s)
+        self.atom_row_host = row
+        dev = self.device
+        self.t_atom_sys = torch.tensor(atom_sys, device=dev)
+        self.t_sys_start = torch.tensor(start, device=dev)
+        self.t_mode = torch.tensor(mode, device=dev)
+        self.t_cell = torch.tensor(cell_arr.reshape(B, 9), device=dev)
+        self.t_recip = torch.tensor(recip_arr.reshape(B, 9), device=dev)
+        self.t_species = torch.tensor(species_idx, device=dev)
+        self.t_atom_row = torch.tensor(row, device=dev)
+        self.t_tile_species = torch.tensor(np.asarray(tiles_s, np.int32), device=dev)
+        self.t_tile_row = torch.tensor(np.asarray(tiles_r, np.int32), device=dev)
+        self._plans: Dict[float, Tuple[torch.Tensor, torch.Tensor, int]] = {}
+
+    def plan(self, cutoff: float):
+        """Cell grid for a cutoff (``fennol_graph_plan``), cached."""
+        key = float(cutoff)
+        if key not in self._plans:
+            import ctypes as C
+            grid = np.zeros((self.nsys, 4), np.int32)
+            nrep = np.zeros((self.nsys, 3), np.int32)
+            total = call("fennol_graph_plan", self.nsys, self.mode_host.ctypes.data,
+                         self.recip_host.ctypes.data, key, grid.ctypes.data, nrep.ctypes.data)
+            self._plans[key] = (torch.tensor(grid, device=self.device),
+                                torch.tensor(nrep, device=self.device), int(total))
+        return self._plans[key]
+
+    def estimate_capacity(self, cutoff: float) -> int:
+        """Initial row length: the largest system size for molecules, the
+        density estimate with a 25% margin for periodic boxes."""
+        best = 8
+        for b in range(self.nsys):
+            nb = int(self.natoms[b])
+            if self.mode_host[b] == 0:
+                best = max(best, nb - 1)
+            else:
+                vol = abs(float(np.linalg.det(self.cell_host[b].astype(np.float64))))
+                est = 4.0 / 3.0 * math.pi * cutoff ** 3 * nb / max(vol, 1e-9)
+                best = max(best, int(est * 1.25) + 16)
+        return min(_ceil(max(best, 8), 8), 1024)
+
+
+class GraphBuffers:
+    """Neighbour rows of one layout: the build list (cutoff + skin) and, when
+    a skin is used, the radial list filtered from it."""
+
+    def __init__(self, layout: BatchLayout, cutoff: float, skin: float, cap: int, cap_radial: int):
+        dev = layout.device
+        n = max(layout.n, 1)
+        self.cutoff, self.skin = cutoff, skin
+        self.cap = cap
+        self.nbr_j = torch.zeros((n, cap), dtype=torch.int32, device=dev)
+        self.nbr_s = torch.zeros((n, cap), dtype=torch.int32, device=dev)
+        self.nbr_n = torch.zeros(n, dtype=torch.int32, device=dev)
+        grid, nrep, ncells = layout.plan(cutoff + skin)
+        self.grid, self.nrep, self.ncells = grid, nrep, ncells
+        ws = _lib.load().fennol_graph_workspace_bytes(n, ncells)
+        self.ws = torch.zeros(int(ws), dtype=torch.uint8, device=dev)
+        if skin > 0:
+            self.cap_r = cap_radial
+            self.rad_j = torch.zeros((n, cap_radial), dtype=torch.int32, device=dev)
+            self.rad_s = torch.zeros((n, cap_radial), dtype=torch.int32, device=dev)
+            self.rad_n = torch.zeros(n, dtype=torch.int32, device=dev)
+        else:
+            self.cap_r = cap
+            self.rad_j, self.rad_s, self.rad_n = self.nbr_j, self.nbr_s, self.nbr_n
+
+    def build(self, layout: BatchLayout, coords: torch.Tensor, status: torch.Tensor, stream: int,
+              enable_flag: Optional[torch.Tensor] = None):
+        call("fennol_graph_build", coords.data_ptr(), layout.n, layout.t_atom_sys.data_ptr(), layout.nsys,
+             layout.t_sys_start.data_ptr(), layout.t_mode.data_ptr(), layout.t_cell.data_ptr(),
+             layout.t_recip.data_ptr(), self.grid.data_ptr(), self.nrep.data_ptr(), self.ncells,
+             float(self.cutoff + self.skin), self.cap, self.nbr_j.data_ptr(), self.nbr_s.data_ptr(),
+             self.nbr_n.data_ptr(), status.data_ptr(), self.ws.data_ptr(), self.ws.numel(),
+             _ptr(enable_flag), stream)
+
+    def filter(self, layout: BatchLayout, coords: torch.Tensor, status: torch.Tensor, stream: int):
+        if self.skin <= 0:
+            return
+        call("fennol_graph_filter", coords.data_ptr(), layout.n, layout.t_atom_sys.data_ptr(),
+             layout.t_cell.data_ptr(), self.nbr_j.data_ptr(), self.nbr_s.data_ptr(), self.nbr_n.data_ptr(),
+             self.cap, float(self.cutoff), self.cap_r, self.rad_j.data_ptr(), self.rad_s.data_ptr(),
+             self.rad_n.data_ptr(), status.data_ptr(), stream)
+
+
+class Workspace:
+    """Per-layout device buffers of one energy/force evaluation."""
+
+    def __init__(self, pot: "ANIPotential", layout: BatchLayout):
+        dev = layout.device
+        n = max(layout.n, 1)
+        rows = layout.rows
+        d0 = pot.mlp.dims[0]
+        self.xyzs = torch.zeros((n, 4), dtype=torch.float32, device=dev)
+        if pot.precision == _lib.MLP_FP32:
+            self.x = torch.zeros((rows, d0), dtype=torch.float32, device=dev)
+            self.x_lo = None
+            self.aev_kind = _lib.AEV_F32
+        else:
+            self.x = torch.zeros((rows, d0), dtype=torch.bfloat16, device=dev)
+            self.x_lo = (torch.zeros((rows, d0), dtype=torch.bfloat16, device=dev)
+                         if pot.precision != _lib.MLP_BF16 else None)
+            self.aev_kind = _lib.AEV_BF16 if pot.precision == _lib.MLP_BF16 else _lib.AEV_BF16X2
+        self.dx = torch.zeros((rows, d0), dtype=torch.float32, device=dev)
+        self.e_rows = torch.zeros(rows, dtype=torch.float32, device=dev)
+        mws = _lib.load().fennol_mlp_workspace_bytes(pot.precision, rows, pot.mlp.n_models,
+                                                     pot.mlp.struct)
+        self.mlp_ws = torch.zeros(max(int(mws), 256), dtype=torch.uint8, device=dev)
+        self.forces4 = torch.zeros((n, 4), dtype=torch.float32, device=dev)
+        self.forces = torch.zeros((n, 3), dtype=torch.float32, device=dev)
+        self.energy = torch.zeros(layout.nsys, dtype=torch.float64, device=dev)
+        self.e_atom = torch.zeros(n, dtype=torch.float64, device=dev)
+        self.status = torch.zeros(_lib.STATUS_WORDS, dtype=torch.int32, device=dev)
+
+
+class ANIPotential:
+    """ANI-2x-style potential evaluated by the sm_100a kernels.
+
+    ``precision``: ``"fp32"`` (CUDA-core GEMMs), ``"bf16"``, ``"bf16x2"`` or
+    ``"bf16x3"`` (tcgen05 tensor-core GEMMs with 1, 2 or 3 BF16 products).
+    Energies are returned in Hartree (FeNNol's default model unit) and
+    forces in Hartree/Angstrom, unless ``energy_unit="kcalpermol"``.
+    """
+
+    def __init__(self, aev: AEVConfig = AEVConfig(), mlp: MLPConfig = MLPConfig(),
+                 weights: Optional[Weights] = None, precision: str = "fp32", device="cuda",
+                 seed: int = 0, n_models: int = 1, energy_unit: str = "Ha",
+                 minimum_image: bool = True):
+        if precision not in _lib.PRECISIONS:
+            raise ValueError(f"precision must be one of {list(_lib.PRECISIONS)}")
+        _lib.load()
+        self.device = torch.device(device)
+        if self.device.type != "cuda":
+            raise RuntimeError("ANIPotential runs on CUDA devices only")
+        self.aev_cfg, self.mlp_cfg = aev, mlp
+        if weights is None:
+            weights = init_weights(aev, mlp, seed=seed, n_models=n_models)
+        self.weights = weights
+        self.precision = _lib.PRECISIONS[precision]
+        self.precision_name = precision
+        self.mlp = PackedMLP(weights, aev, mlp, self.device, self.precision)
+        self.params = aev_params(aev)
+        if _lib.load().fennol_aev_length(C_ptr(self.params)) != aev.aev_length:
+            raise ValueError("unsupported AEV hyper-parameters for the CUDA kernels")
+        self.unit_scale = {"ha": 1.0, "hartree": 1.0,
+                           "kcalpermol": HARTREE_TO_KCALMOL}[energy_unit.lower()]
+        self.minimum_image = minimum_image
+        self._cache: Dict[tuple, tuple] = {}
+        self.capacity_margin = 1.05
+        self.add_neigh = 8
+
+    # ------------------------------------------------------------------ layout
+    def layout(self, species, natoms, cells=None) -> BatchLayout:
+        sidx = self.aev_cfg.species_index(np.asarray(species))
+        return BatchLayout(sidx, natoms, cells, self.minimum_image, self.device)
+
+    def buffers(self, layout: BatchLayout, skin: float = 0.0, cap: Optional[int] = None,
+                cap_radial: Optional[int] = None):
+        rc = self.aev_cfg.radial_cutoff
+        if cap is None:
+            cap = layout.estimate_capacity(rc + skin)
+        if cap_radial is None:
+            cap_radial = layout.estimate_capacity(rc) if skin > 0 else cap
+        g = GraphBuffers(layout, rc, skin, cap, cap_radial)
+        ws = Workspace(self, layout)
+        return g, ws
+
+    # --------------------------------------------------------------- launches
+    def launch_forces(self, layout: BatchLayout, g: GraphBuffers, ws: Workspace, stream: int,
+                      want_forces: bool = True):
+        """AEV -> MLP -> energies (and adjoint -> forces) from the current radial list."""
+        lib_p = C_ptr(self.params)
+        n = layout.n
+        call("fennol_aev_forward", ws.xyzs.data_ptr(), n, layout.t_atom_sys.data_ptr(),
+             layout.t_cell.data_ptr(), g.rad_j.data_ptr(), g.rad_s.data_ptr(), g.rad_n.data_ptr(),
+             g.cap_r, lib_p, layout.t_atom_row.data_ptr(), ws.aev_kind, ws.x.data_ptr(),
+             _ptr(ws.x_lo), ws.x.shape[1], ws.status.data_ptr(), stream)
+        call("fennol_mlp_energy_grad", self.precision, layout.rows, layout.ntiles,
+             layout.t_tile_species.data_ptr(), layout.t_tile_row.data_ptr(), C_ptr(self.mlp.struct),
+             ws.x.data_ptr(), _ptr(ws.x_lo), ws.e_rows.data_ptr(), ws.dx.data_ptr(),
+             ws.mlp_ws.data_ptr(), ws.mlp_ws.numel(), stream)
+        call("fennol_energy_reduce", ws.e_rows.data_ptr(), layout.t_atom_row.data_ptr(), n,
+             layout.t_sys_start.data_ptr(), layout.nsys, float(self.unit_scale), ws.energy.data_ptr(),
+             ws.e_atom.data_ptr(), stream)
+        if want_forces:
+            ws.forces4.zero_()
+            call("fennol_aev_backward", ws.xyzs.data_ptr(), n, layout.t_atom_sys.data_ptr(),
+                 layout.t_cell.data_ptr(), g.rad_j.data_ptr(), g.rad_s.data_ptr(), g.rad_n.data_ptr(),
+                 g.cap_r, lib_p, layout.t_atom_row.data_ptr(), ws.dx.data_ptr(), ws.dx.shape[1],
+                 ws.forces4.data_ptr(), ws.status.data_ptr(), stream)
+
+    def check_status(self, ws: Workspace, g: GraphBuffers) -> Optional[Tuple[int, int]]:
+        """None if every list fitted, else the capacities to regrow to."""
+        st = ws.status.cpu().numpy()
+        if st[_lib.ST_ANG_OVERFLOW]:
+            raise RuntimeError(f"more than {_lib.MAX_ANGULAR_NEIGHBORS} angular neighbours "
+                               f"({int(st[_lib.ST_ANG_MAXCOUNT])}) around one atom")
+        grow = None
+        if st[_lib.ST_NBR_OVERFLOW] or st[_lib.ST_FILTER_OVERFLOW]:
+            cap = g.cap
+            capr = g.cap_r
+            if st[_lib.ST_NBR_OVERFLOW]:
+                cap = int(self.capacity_margin * st[_lib.ST_NBR_MAXCOUNT]) + self.add_neigh
+            if st[_lib.ST_FILTER_OVERFLOW]:
+                capr = int(self.capacity_margin * st[_lib.ST_FILTER_MAXCOUNT]) + self.add_neigh
+            if g.skin <= 0:
+                capr = cap
+            if max(cap, capr) > 1024:
+                raise RuntimeError("neighbour rows longer than 1024 are not supported")
+            grow = (_ceil(cap, 8), _ceil(capr, 8))
+        return grow
+
+    def _get(self, key, layout_fn):
+        if key not in self._cache:
+            layout = layout_fn()
+            g, ws = self.buffers(layout)
+            self._cache = {key: (layout, g, ws)}  # one cached layout
+        return self._cache[key]
+
+    def energy_and_forces(self, coordinates, species, natoms=None, cells=None,
+                          want_forces: bool = True):
+        """Energies [B] (float64) and forces [N,3] (float32) as torch tensors
+        on the device.  ``coordinates`` may be a host array or a device
+        tensor ([N,3], Angstrom); ``species`` are atomic numbers."""
+        species = np.asarray(species)
+        if natoms is None:
+            natoms = [species.shape[0]]
+        natoms = tuple(int(v) for v in np.asarray(natoms).reshape(-1))
+        if cells is None:
+            cell_key = None
+        elif isinstance(cells, (list, tuple)):
+            cell_key = tuple(None if c is None else np.asarray(c, np.float32).tobytes() for c in cells)
+        else:
+            cell_key = np.asarray(cells, dtype=np.float32).tobytes()
+        key = (species.tobytes(), natoms, cell_key)
+        layout, g, ws = self._get(key, lambda: self.layout(species, natoms, cells))
+        coords = torch.as_tensor(coordinates, dtype=torch.float32)
+        if coords.device != self.device:
+            coords = coords.to(self.device, non_blocking=True)
+        coords = coords.contiguous()
+        stream = _stream(self.device)
+        for _attempt in range(4):
+            ws.status.zero_()
+            call("fennol_pack_atoms", coords.data_ptr(), layout.t_species.data_ptr(), layout.n,
+                 ws.xyzs.data_ptr(), stream)
+            g.build(layout, coords, ws.status, stream)
+            g.filter(layout, coords, ws.status, stream)
+            self.launch_forces(layout, g, ws, stream, want_forces)
+            grow = self.check_status(ws, g)
+            if grow is None:
+                break
+            g = GraphBuffers(layout, g.cutoff, g.skin, grow[0], grow[1])
+            self._cache[key] = (layout, g, ws)
+        else:
+            raise RuntimeError("neighbour capacity did not converge")
+        forces = None
+        if want_forces:
+            call("fennol_forces_finalize", ws.forces4.data_ptr(), layout.n, float(self.unit_scale),
+                 ws.forces.data_ptr(), stream)
+            forces = ws.forces
+        return ws.energy, forces
+
+    def neighbor_lists(self, coordinates, species, natoms=None, cells=None, cutoff=None):
+        """Per-atom rows (j, shift, count) of the pair list for ``cutoff``
+        (default: the radial cutoff) as host arrays, regrowing on overflow."""
+        species = np.asarray(species)
+        if natoms is None:
+            natoms = [species.shape[0]]
+        layout = self.layout(species, natoms, cells)
+        rc = self.aev_cfg.radial_cutoff if cutoff is None else cutoff
+        cap = layout.estimate_capacity(rc)
+        coords = torch.as_tensor(np.asarray(coordinates), dtype=torch.float32).to(self.device).contiguous()
+        status = torch.zeros(_lib.STATUS_WORDS, dtype=torch.int32, device=self.device)
+        stream = _stream(self.device)
+        for _ in range(4):
+            g = GraphBuffers(layout, rc, 0.0, cap, cap)
+            status.zero_()
+            g.build(layout, coords, status, stream)
+            st = status.cpu().numpy()
+            if not st[_lib.ST_NBR_OVERFLOW]:
+                return g.nbr_j.cpu().numpy(), g.nbr_s.cpu().numpy(), g.nbr_n.cpu().numpy(), layout
+            cap = _ceil(int(1.05 * st[_lib.ST_NBR_MAXCOUNT]) + 8, 8)
+        raise RuntimeError("neighbour capacity did not converge")
+
+
+def C_ptr(struct):
+    import ctypes
+    return ctypes.pointer(struct)
+
+
+def unpack_shifts(packed: np.ndarray) -> np.ndarray:
+    """Packed signed-byte shifts (x | y<<8 | z<<16) -> int [..., 3]."""
+    p = np.asarray(packed).astype(np.int64) & 0xFFFFFF
+    out = np.stack([(p >> (8 * k)) & 0xFF for k in range(3)], -1)
+    return np.where(out >= 128, out - 256, out)

@@ -1,0 +1,296 @@
+/*
+ * fennol_b200 -- C ABI of the B200 (sm_100a) energy-and-force path of an
+ * ANI-2x-style potential.
+ *
+ * Conventions shared by every entry point:
+ *   - all array pointers are DEVICE pointers unless the name says host_;
+ *   - the library allocates nothing: the caller passes every output and
+ *     workspace buffer (sizes come from the *_bytes queries);
+ *   - `stream` is a cudaStream_t passed as void*; every launch is enqueued
+ *     on it and nothing synchronises the device;
+ *   - return value: FENNOL_OK (0) or a negative FENNOL_ERR_* code; nothing
+ *     aborts and nothing throws.  Capacity problems found on the device are
+ *     reported through the int32 `status` words (see FENNOL_ST_*), like the
+ *     reference's `overflow` flags, and the caller regrows and relaunches;
+ *   - atoms of one system are contiguous; `atom_sys[i]` is FeNNol's
+ *     `batch_index`, `sys_start[b]` the first atom of system b;
+ *   - cells are row-major 3x3, rows are lattice vectors (FeNNol `cells[b]`);
+ *     a periodic image of atom j is x_j + shift @ cell.
+ *
+ * Reference interfaces named below are files of thomasple/FeNNol.
+ */
+#ifndef FENNOL_B200_H
+#define FENNOL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FENNOL_OK 0
+#define FENNOL_ERR_INVALID (-1)
+#define FENNOL_ERR_CUDA (-2)
+#define FENNOL_ERR_UNSUPPORTED (-3)
+#define FENNOL_ERR_WORKSPACE (-4)
+
+#define FENNOL_STATUS_WORDS 8
+#define FENNOL_ST_NBR_OVERFLOW 0
+#define FENNOL_ST_NBR_MAXCOUNT 1
+#define FENNOL_ST_FILTER_OVERFLOW 2
+#define FENNOL_ST_FILTER_MAXCOUNT 3
+#define FENNOL_ST_ANG_OVERFLOW 4
+#define FENNOL_ST_ANG_MAXCOUNT 5
+#define FENNOL_ST_CELL_OVERFLOW 6
+#define FENNOL_ST_REBUILD_COUNT 7
+
+/* Periodic handling of one system (GraphGenerator, preprocessing.py:117-258). */
+#define FENNOL_PBC_NONE 0
+#define FENNOL_PBC_MINIMUM_IMAGE 1
+#define FENNOL_PBC_GENERAL 2
+
+/* Largest number of in-kernel angular neighbours per centre atom. */
+#define FENNOL_MAX_ANGULAR_NEIGHBORS 96
+
+/* ------------------------------------------------------------------------ */
+/* Library                                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* Version string of the build. */
+const char* fennol_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Neighbour search                                                          */
+/* ------------------------------------------------------------------------ */
+
+/*
+ * Host-only planning of the cell grid for each system.  Replaces the shape
+ * bookkeeping of GraphGenerator.__call__ (preprocessing.py:90-100, 168-182):
+ * for periodic systems whose cell holds at least 3 bins of width > cutoff
+ * along every axis the builder uses a cell list, otherwise it tests all pairs
+ * (with image repeats ceil(cutoff*|recip column|) for general PBC).
+ *   host_mode[nsys], host_recip[nsys*9]: inputs;
+ *   host_grid[nsys*4] out: (nx, ny, nz, first global cell) or zeros;
+ *   host_nrep[nsys*3] out: image repeats for all-pairs general PBC;
+ *   returns the total number of cells (>= 0) or a negative error.
+ */
+int fennol_graph_plan(int nsys, const int* host_mode, const float* host_recip, double cutoff,
+                      int* host_grid, int* host_nrep);
+
+/* Workspace of fennol_graph_build, in bytes. */
+size_t fennol_graph_workspace_bytes(int natoms, int ncells_total);
+
+/*
+ * Periodic cell-list neighbour search.  Replaces GraphGenerator.__call__ and
+ * GraphGenerator.process (preprocessing.py:74-355, 369-638).
+ *
+ * For every atom i it writes the row of all j != i of the same system (and
+ * periodic image) with d^2 < cutoff^2, where d^2 is computed exactly like the
+ * reference's float32 numpy path: vec = x_j - x_i, minimum image
+ * s = -rint(vec @ recip), vec += s @ cell, d^2 = (x*x + y*y) + z*z, compared
+ * with (float)(cutoff*cutoff) (cutoff is passed in double precision so the
+ * threshold rounds exactly like the reference's Python float).  General PBC wraps atoms with -floor(x @ recip)
+ * first and stores shift = image + at_shift[j] - at_shift[i] (:340-346).
+ * Rows are sorted by (j, shift), so the result is deterministic.
+ * Outputs: nbr_j[natoms*capacity], nbr_shift[natoms*capacity] (packed
+ * signed bytes x | y<<8 | z<<16), nbr_count[natoms] (clamped to capacity).
+ * Overflow sets status[FENNOL_ST_NBR_OVERFLOW] and the needed row length goes
+ * to status[FENNOL_ST_NBR_MAXCOUNT] (the reference's check_reallocate,
+ * preprocessing.py:357-367).  If `enable_flag` is not NULL the launch does
+ * nothing unless *enable_flag != 0 (device-side rebuild trigger); on a
+ * rebuild it increments status[FENNOL_ST_REBUILD_COUNT].
+ */
+int fennol_graph_build(const float* coords, int natoms, const int* atom_sys, int nsys,
+                       const int* sys_start, const int* sys_mode, const float* sys_cell,
+                       const float* sys_recip, const int* sys_grid, const int* sys_nrep,
+                       int ncells_total, double cutoff, int capacity, int* nbr_j,
+                       unsigned* nbr_shift, int* nbr_count, int* status, void* workspace,
+                       size_t workspace_bytes, const int* enable_flag, void* stream);
+
+/*
+ * Re-filter a neighbour list to a smaller cutoff from current positions.
+ * Replaces GraphGenerator.update_skin (preprocessing.py:640-696) when applied
+ * to the skin list, and GraphFilter (preprocessing.py:834-960) when applied
+ * to the radial list with the angular cutoff.  vec = (x_j - x_i) + s @ cell
+ * with the same float32 arithmetic; kept rows preserve the input order.
+ */
+int fennol_graph_filter(const float* coords, int natoms, const int* atom_sys,
+                        const float* sys_cell, const int* in_j, const unsigned* in_shift,
+                        const int* in_count, int in_capacity, double cutoff, int out_capacity,
+                        int* out_j, unsigned* out_shift, int* out_count, int* status,
+                        void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* ANI atomic environment vectors                                            */
+/* ------------------------------------------------------------------------ */
+
+/* Hyper-parameters of ANIAEV (embeddings/ani.py:18-44). */
+typedef struct fennol_aev_params {
+  int num_species;          /* S <= 8 */
+  int radial_divisions;     /* 16 or 32 */
+  int angular_divisions;    /* angular_dist_divisions */
+  int angle_sections;       /* angular_divisions * angle_sections == 32 */
+  double radial_cutoff;
+  double angular_cutoff;
+  float radial_eta;
+  float angular_eta;
+  float zeta;
+  float radial_start;
+  float angular_start;
+} fennol_aev_params;
+
+/* AEV width S*RD + S(S+1)/2*AD*AS, or -1 for unsupported parameters. */
+int fennol_aev_length(const fennol_aev_params* p);
+
+/*
+ * Pack positions and species for the AEV kernels: xyzs[i] = (x, y, z,
+ * species index as int bits).  species_idx are positions in species_order.
+ */
+int fennol_pack_atoms(const float* coords, const int* species_idx, int natoms, float* xyzs,
+                      void* stream);
+
+/* AEV output encodings. */
+#define FENNOL_AEV_F32 0     /* float32 rows */
+#define FENNOL_AEV_BF16 1    /* bfloat16 rows */
+#define FENNOL_AEV_BF16X2 2  /* bfloat16 hi rows + bfloat16 lo rows (x ~= hi + lo) */
+
+/*
+ * ANIAEV forward.  Replaces ANIAEV.__call__ (embeddings/ani.py:47-142) with
+ * the graph processors it reads (GraphProcessor preprocessing.py:719-777,
+ * GraphFilterProcessor :979-1043, GraphAngularExtension :1085-1276,
+ * GraphAngleProcessor :1294-1317, SwitchFunction misc/misc.py:617-716).
+ * nbr_* is the radial list (cutoff p->radial_cutoff); the angular neighbours
+ * (d^2 < angular_cutoff^2 with the reference's float32 arithmetic) and all
+ * their unordered pairs (the triplets) are formed on chip.
+ * Row i of the output is written at row `atom_row[i]` of `out` (leading
+ * dimension `ld` elements); columns [F, ld) are left untouched.
+ */
+int fennol_aev_forward(const float* xyzs, int natoms, const int* atom_sys, const float* sys_cell,
+                       const int* nbr_j, const unsigned* nbr_shift, const int* nbr_count,
+                       int capacity, const fennol_aev_params* p, const int* atom_row,
+                       int out_kind, void* out, void* out_lo, int ld, int* status, void* stream);
+
+/*
+ * Adjoint of fennol_aev_forward: given dE/dAEV (float32 rows at atom_row,
+ * leading dimension ld) accumulate forces -dE/dx into forces4[natoms*4]
+ * (x, y, z, unused).  Replaces the reverse-mode transpose of the AEV
+ * (jax.grad through ani.py and the graph processors, fennix.py:260-272).
+ * forces4 must be zeroed (or hold other force terms) before the call.
+ */
+int fennol_aev_backward(const float* xyzs, int natoms, const int* atom_sys,
+                        const float* sys_cell, const int* nbr_j, const unsigned* nbr_shift,
+                        const int* nbr_count, int capacity, const fennol_aev_params* p,
+                        const int* atom_row, const float* daev, int ld, float* forces4,
+                        int* status, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Species-indexed MLP                                                       */
+/* ------------------------------------------------------------------------ */
+
+#define FENNOL_MLP_FP32 0     /* float32 CUDA-core GEMMs */
+#define FENNOL_MLP_BF16 1     /* tcgen05 BF16 x BF16, FP32 accumulate */
+#define FENNOL_MLP_BF16X2 2   /* activations split hi+lo BF16 (2 MMAs); weights as BF16 */
+#define FENNOL_MLP_BF16X3 3   /* activations and weights split (3 MMAs) */
+
+#define FENNOL_MLP_LAYERS 4
+
+/*
+ * Packed weights of an ensemble of per-species networks
+ * (FullyConnectedNet, misc/nets.py:13-102, inside SpeciesIndexNet :301-426).
+ * A "group" is (model m, species s), index g = m*n_species + s.
+ * dims[0..4] are the zero-padded widths (multiples of 64 except dims[4]=1):
+ * 1024, 256, 192, 192, 1 for the ANI-2x network 1008-256-192-160-1.
+ *   w32[l]: float32 [G][dims[l]][dims[l+1]]  (kernel, zero padded)
+ *   b32[l]: float32 [G][dims[l+1]]
+ *   wt_hi[l], wt_lo[l]: bfloat16 [G][dims[l+1]][dims[l]]  (kernel^T, K-major)
+ *   w_hi[l], w_lo[l]:   bfloat16 [G][dims[l]][dims[l+1]]  (kernel, K-major for the
+ *                        input-gradient GEMMs); used for l = 0..2.
+ * bf16 pointers may be NULL for FENNOL_MLP_FP32; *_lo may be NULL unless
+ * FENNOL_MLP_BF16X3.
+ */
+typedef struct fennol_mlp_weights {
+  int n_models;
+  int n_species;
+  int dims[5];
+  float celu_alpha;
+  const float* w32[FENNOL_MLP_LAYERS];
+  const float* b32[FENNOL_MLP_LAYERS];
+  const void* wt_hi[FENNOL_MLP_LAYERS];
+  const void* wt_lo[FENNOL_MLP_LAYERS];
+  const void* w_hi[FENNOL_MLP_LAYERS];
+  const void* w_lo[FENNOL_MLP_LAYERS];
+} fennol_mlp_weights;
+
+/* Workspace of fennol_mlp_energy_grad for `rows` padded rows, in bytes. */
+size_t fennol_mlp_workspace_bytes(int precision, int rows, int n_models,
+                                  const fennol_mlp_weights* w);
+
+/*
+ * Energies and input gradients of the species networks.  Replaces the
+ * SpeciesIndexNet forward (nets.py:397-417), its jax.grad transpose and the
+ * ensemble mean.  Rows are grouped by species in tiles of 128: tile t covers
+ * rows [tile_row[t], tile_row[t]+128) of species tile_species[t] (padding
+ * rows must hold zeros).  Inputs: x (AEV rows, ld = dims[0]; float32 for
+ * FENNOL_MLP_FP32, bfloat16 hi (+ lo) otherwise).  Outputs: e_rows[rows]
+ * (ensemble-mean atomic energy) and dx[rows*dims[0]] (float32 dE/dAEV,
+ * ensemble mean).
+ */
+int fennol_mlp_energy_grad(int precision, int rows, int ntiles, const int* tile_species,
+                           const int* tile_row, const fennol_mlp_weights* w, const void* x,
+                           const void* x_lo, float* e_rows, float* dx, void* workspace,
+                           size_t workspace_bytes, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Reductions and outputs                                                    */
+/* ------------------------------------------------------------------------ */
+
+/*
+ * Per-system energies in float64: energy[b] = scale * sum_{i in b}
+ * e_rows[atom_row[i]] (fixed summation order).  Replaces the segment_sum of
+ * FENNIX.total_energy (fennix.py:218-258).  e_atom (float64 [natoms], may be
+ * NULL) receives scale * per-atom energies in input order.
+ */
+int fennol_energy_reduce(const float* e_rows, const int* atom_row, int natoms,
+                         const int* sys_start, int nsys, double scale, double* energy,
+                         double* e_atom, void* stream);
+
+/* forces[i*3+k] = scale * forces4[i*4+k] (float32 output). */
+int fennol_forces_finalize(const float* forces4, int natoms, float scale, float* forces,
+                           void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Molecular dynamics                                                        */
+/* ------------------------------------------------------------------------ */
+
+/*
+ * One BAOAB-style step of FeNNol's integrator (md/integrate.py:286-294) in
+ * float64:  v += dt/m * F;  x += dt/2 v;  v = a1 v + a2_i xi (Langevin,
+ * thermostats.py:56-120; NVE when a1 == 1 and a2 == NULL);  x += dt/2 v.
+ * Units: A, ps, kcal/mol; inv_mass[i] = 1/m_i in the same system; forces4
+ * holds -dE/dx in model units and is multiplied by force_scale.  xi are
+ * standard normal numbers from a counter-based Philox4x32-10 stream keyed by
+ * (seed, step).  Also writes float32 positions (coords) and packed xyzs for
+ * the next force call, and sets *rebuild_flag = 1 when an atom moved more
+ * than half the skin since the last rebuild (x_ref).  If rebuild_flag is
+ * NULL no displacement check is done.
+ */
+int fennol_md_step(int natoms, double dt, double* x, double* v, const double* inv_mass,
+                   const float* forces4, double force_scale, double a1, const double* a2,
+                   unsigned long long seed, unsigned long long step, float* coords,
+                   const int* species_idx, float* xyzs, const double* x_ref, double half_skin,
+                   int* rebuild_flag, void* stream);
+
+/* After a rebuild: x_ref = x and *rebuild_flag = 0 (both device). */
+int fennol_md_mark_rebuilt(int natoms, const double* x, double* x_ref, int* rebuild_flag,
+                           void* stream);
+
+/* kinetic[0] = 0.5 * sum m v^2 (float64, deterministic order). */
+int fennol_md_kinetic(int natoms, const double* v, const double* inv_mass, double* kinetic,
+                      void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FENNOL_B200_H */
