@@ -1,0 +1,376 @@
+"""Benchmark of the ANI-2x energy+force MD step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload water12k|water98k] [--precision bf16x3|bf16x2|bf16|fp32]
+
+A step is one MD step of the workload: BAOAB integrator (float64) ->
+neighbour list (skin filter every step, cell-list rebuild when an atom moved
+more than half the skin) -> AEV -> species MLPs -> energy -> force adjoint,
+replayed from a CUDA graph.  Inputs live in HBM; every timed step is
+bracketed by CUDA events on the launching stream and preceded by an L2 flush
+(a 512 MB write) outside the events.  Multi-GPU runs (torchrun) are
+independent replicas (weak scaling); the time is the max over ranks.
+Prints one JSON line on rank 0.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "E+F atom-steps/s (1 B200, BF16 vs FP32 form) at stated force RMSE; p50/p99 latency"
+HARTREE_TO_KCALMOL = 627.5096080305927
+MLP_FLOP_PER_ATOM = 2 * (1008 * 256 + 256 * 192 + 192 * 160 + 160 * 1) * 2  # fwd + input grad
+
+WORKLOADS = {
+    "water12k": dict(n_side=16, n_models=1, thermostat="LGV", desc=(
+        "water box 12,288 atoms (4096 H2O, 49.7 A cube), Langevin 300 K gamma 1/ps, dt 0.5 fs, "
+        "skin 1.0 A with displacement-triggered rebuild, ANI-2x 7-species random-init model "
+        "(MD: last layer x0.02)")),
+    "water98k": dict(n_side=32, n_models=8, thermostat="NVE", desc=(
+        "water box 98,304 atoms (32768 H2O, 99.4 A cube), NVE dt 0.5 fs, skin 1.0 A, "
+        "8-model ANI-2x ensemble (random-init, MD: last layer x0.02)")),
+}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}", "--format=csv,noheader",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1].split()[0]))
+                mx = float(f[2].split()[0])
+            except ValueError:
+                continue
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return d["hbm_gbs"], d["bf16_tflops"], d.get("bf16_tflops_sustained"), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, 1590.0, 1400.0, "fallback"
+
+
+def make_engine(workload, precision, device, seed=0):
+    from fennol_b200.md import MDEngine
+    from fennol_b200.potential import ANIPotential
+    from fennol_b200.systems import water_box
+
+    from fennol_b200.params import MD_OUTPUT_SCALE
+
+    w = WORKLOADS[workload]
+    box = water_box(w["n_side"], seed=seed)
+    pot = ANIPotential(precision=precision, device=device, seed=0, n_models=w["n_models"],
+                       output_scale=MD_OUTPUT_SCALE)
+    eng = MDEngine(pot, box.coordinates, box.species, box.cell, dt_fs=0.5, thermostat=w["thermostat"],
+                   temperature=300.0, gamma_ps=1.0, skin=1.0, trigger="displacement", seed=seed)
+    return box, pot, eng
+
+
+def time_steps(eng, steps, warmup, flush):
+    """Per-step device times (ms) of graph-replayed MD steps, L2 flushed between steps."""
+    import torch
+
+    eng.run(warmup)  # also regrows lists if needed
+    graph = eng._graph_for(None, 1)
+    stream = torch.cuda.current_stream()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    eng.snapshot()
+    torch.cuda.synchronize()
+    for k in range(steps):
+        flush.zero_()
+        starts[k].record(stream)
+        graph.replay()
+        ends[k].record(stream)
+    torch.cuda.synchronize()
+    if eng._regrow():  # an overflow during timing: lists regrown, time again
+        return time_steps(eng, steps, 0, flush)
+    eng.step_count += steps
+    return np.array([s.elapsed_time(e) for s, e in zip(starts, ends)])
+
+
+def time_mlp(pot, eng, reps):
+    """Average duration (ms) of the species-MLP launch on the current state."""
+    import torch
+    from fennol_b200._lib import call
+    from fennol_b200.potential import C_ptr, _ptr
+
+    lay, ws = eng.layout, eng.ws
+    st = torch.cuda.current_stream().cuda_stream
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def launch():
+        call("fennol_mlp_energy_grad", pot.precision, lay.rows, lay.ntiles, lay.t_tile_species.data_ptr(),
+             lay.t_tile_row.data_ptr(), C_ptr(pot.mlp.struct), ws.x.data_ptr(), _ptr(ws.x_lo),
+             ws.e_rows.data_ptr(), ws.dx.data_ptr(), ws.mlp_ws.data_ptr(), ws.mlp_ws.numel(), st)
+
+    for _ in range(3):
+        launch()
+    torch.cuda.synchronize()
+    ev0.record()
+    for _ in range(reps):
+        launch()
+    ev1.record()
+    torch.cuda.synchronize()
+    return ev0.elapsed_time(ev1) / reps
+
+
+def accuracy(pot, box):
+    """Single-point error of this precision vs the FP64 oracle."""
+    from oracle import ani_ref
+
+    e, f = pot.energy_and_forces(box.coordinates, box.species, [box.natoms], box.cell[None])
+    ref = ani_ref.energy_and_forces(box.coordinates, box.species, [box.natoms], pot.weights,
+                                    pot.aev_cfg, pot.mlp_cfg, cells=box.cell[None])
+    de = abs(float(e[0]) - ref["energy"][0]) * HARTREE_TO_KCALMOL / box.natoms
+    rmse = float(np.sqrt(np.mean((f.cpu().numpy() - ref["forces"]) ** 2)) * HARTREE_TO_KCALMOL)
+    return {"force_rmse_kcalmol_A": rmse, "energy_err_kcalmol_atom": de,
+            "force_rmse_tol": 0.05, "energy_tol": 1e-4}
+
+
+def e2e(pot, box, steps, warmup):
+    """Public API call per step with pinned host coordinates in and host
+    forces/energy out (single point: the neighbour list is rebuilt each call)."""
+    import torch
+
+    x_host = torch.tensor(box.coordinates, dtype=torch.float32).pin_memory()
+    f_host = torch.empty((box.natoms, 3), dtype=torch.float32).pin_memory()
+    e_host = torch.empty(1, dtype=torch.float64).pin_memory()
+    dev = pot.device
+    x_dev = torch.empty_like(x_host, device=dev)
+    for _ in range(warmup):
+        x_dev.copy_(x_host, non_blocking=True)
+        e, f = pot.energy_and_forces(x_dev, box.species, [box.natoms], box.cell[None])
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(steps):
+        x_dev.copy_(x_host, non_blocking=True)
+        e, f = pot.energy_and_forces(x_dev, box.species, [box.natoms], box.cell[None])
+        f_host.copy_(f, non_blocking=True)
+        e_host.copy_(e[:1], non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+    t1.record()
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1) / steps
+    return {"value": box.natoms / (ms * 1e-3), "unit": "atom-steps/s", "ms_per_step": ms,
+            "h2d_bytes_per_step": int(x_host.numel() * 4),
+            "d2h_bytes_per_step": int(f_host.numel() * 4 + 8),
+            "api": "ANIPotential.energy_and_forces (single point, list rebuilt every call)"}
+
+
+def cpu_baseline(box, n_models, samples=1):
+    """The CPU oracle (float32 torch restatement of the reference formulas,
+    numpy float32 pair search) timed on this host's cores."""
+    import torch
+    from fennol_b200.params import AEVConfig, MLPConfig, init_weights
+    from oracle import ani_ref
+
+    cores = os.cpu_count() or 1
+    torch.set_num_threads(cores)
+    cfg, mcfg = AEVConfig(), MLPConfig()
+    W = init_weights(cfg, mcfg, seed=0, n_models=n_models)
+    ts = []
+    for _ in range(samples):
+        t = time.perf_counter()
+        ani_ref.energy_and_forces(box.coordinates, box.species, [box.natoms], W, cfg, mcfg,
+                                  cells=box.cell[None], dtype=torch.float32)
+        ts.append(time.perf_counter() - t)
+    sec = float(np.median(ts))
+    return {"value": box.natoms / sec, "unit": "atom-steps/s", "cores": cores, "kind": "port",
+            "sample": (f"{samples} single-point E+F of the {box.natoms}-atom box "
+                       f"(pair search + AEV + {n_models}-model MLP + autodiff forces), "
+                       f"float32, {sec:.2f} s each")}
+
+
+def run_reference(args):
+    """Reference arm: the CPU restatement of the reference algorithm, one
+    bounded MD-step sample per timed step, rank 0 only."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from fennol_b200.systems import water_box
+    w = WORKLOADS[args.workload]
+    box = water_box(w["n_side"], seed=0)
+    steps = max(1, min(args.steps, 3))
+    base = cpu_baseline(box, w["n_models"], samples=steps)
+    line = {"metric": METRIC, "value": base["value"], "unit": "atom-steps/s", "n_gpus": world,
+            "steps": steps, "warmup": 0, "ms_per_step": box.natoms / base["value"] * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": w["desc"]},
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": "atom-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "note": ("the reference (JAX/Flax) is not installed in this image; its CPU path is "
+                     "restated by the oracle and timed on the host cores")}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="water12k", choices=list(WORKLOADS))
+    ap.add_argument("--precision", default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = dist_env()
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", device_id=torch.device(f"cuda:{local}"),
+                                timeout=__import__("datetime").timedelta(seconds=300))
+    device = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(device)
+
+    from fennol_b200 import _lib
+    precision = args.precision
+    if precision is None:
+        precision = "bf16x3" if os.environ.get("FENNOL_BENCH_FP32_ONLY") is None else "fp32"
+    w = WORKLOADS[args.workload]
+    try:
+        box, pot, eng = make_engine(args.workload, precision, device, seed=rank)
+    except _lib.FennolError as err:
+        if err.code != _lib.ERR_UNSUPPORTED:
+            raise
+        precision = "fp32"
+        box, pot, eng = make_engine(args.workload, precision, device, seed=rank)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        ms = time_steps(eng, args.steps, args.warmup, flush)
+    total_ms = float(ms.sum())
+    if world > 1:
+        t = torch.tensor([total_ms], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t)
+        dist.barrier()
+    value = world * box.natoms * args.steps / (total_ms * 1e-3)
+
+    res = {"metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "bf16" if precision.startswith("bf16") else "f32", "data": "synthetic",
+           "config": {"workload": w["desc"], "atoms_per_gpu": box.natoms, "precision": precision,
+                      "mlp_precision": {"fp32": "float32 CUDA cores",
+                                        "bf16": "tcgen05 BF16, FP32 accumulate",
+                                        "bf16x2": "tcgen05 BF16 hi+lo activations (2 MMAs)",
+                                        "bf16x3": "tcgen05 BF16 hi+lo activations and weights (3 MMAs)"}[precision],
+                      "aev": "float32", "integrator": "float64",
+                      "l2": "flushed between timed steps (512 MB write outside the events)",
+                      "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+           "latency_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99))},
+           "clocks": clocks.summary(),
+           "gpu_launches": eng.launches_per_step() * args.steps,
+           "rebuilds_in_run": eng.rebuild_count()}
+    if rank == 0:
+        hbm, tf_burst, tf_sust, src = measured_peaks()
+        mlp_ms = time_mlp(pot, eng, 20)
+        flops = MLP_FLOP_PER_ATOM * box.natoms * w["n_models"]
+        achieved = flops / (mlp_ms * 1e-3) / 1e12
+        res["roofline"] = {"bound": "tensor", "kernel": "species MLP (fennol_mlp_energy_grad)",
+                           "achieved": achieved, "peak": tf_burst, "unit": "TFLOP/s",
+                           "frac": achieved / tf_burst, "peak_source": f"{src} bf16 burst",
+                           "algorithmic_flop_per_launch": flops, "ms_per_launch": mlp_ms,
+                           "traffic": None}
+        if precision != "fp32":
+            _, pot32, eng32 = make_engine(args.workload, "fp32", device, seed=rank)
+            ms32 = time_steps(eng32, max(5, args.steps // 3), 3, flush)
+            v32 = box.natoms / (float(ms32.mean()) * 1e-3)
+            res["fp32_form"] = {"value": v32, "ms_per_step": float(ms32.mean()),
+                                "mlp_ms_per_launch": time_mlp(pot32, eng32, 10)}
+            res["speedup_vs_fp32_form"] = value / world / v32
+            del eng32, pot32
+        from fennol_b200.potential import ANIPotential
+        spec = ANIPotential(precision=precision, device=device, seed=0, n_models=w["n_models"])
+        res["accuracy_vs_fp64_oracle"] = accuracy(spec, box)
+        res["accuracy_vs_fp64_oracle"]["model"] = "unscaled N(0, 1/fan_in) random-init weights"
+        del spec
+        res["e2e"] = e2e(pot, box, max(5, args.steps // 3), 3)
+        if not args.no_cpu_baseline:
+            res["cpu_baseline"] = cpu_baseline(box, w["n_models"])
+        print(json.dumps(res), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

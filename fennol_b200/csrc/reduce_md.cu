@@ -76,7 +76,8 @@ __device__ __forceinline__ void box_muller(unsigned a, unsigned b, double& z0, d
 __global__ void k_md_step(int n, double dt, double* __restrict__ x, double* __restrict__ v,
                           const double* __restrict__ inv_mass, const float4* __restrict__ f4,
                           double fscale, double a1, const double* __restrict__ a2,
-                          unsigned long long seed, unsigned long long step, float* __restrict__ coords,
+                          unsigned long long seed, const unsigned long long* __restrict__ step_counter,
+                          float* __restrict__ coords,
                           const int* __restrict__ sp, float4* __restrict__ xyzs,
                           const double* __restrict__ x_ref, double half_skin2, int* rebuild_flag) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -96,6 +97,7 @@ __global__ void k_md_step(int n, double dt, double* __restrict__ x, double* __re
   pz += h * vz;
   // O: Langevin
   if (a2) {
+    unsigned long long step = *step_counter;
     U4 r = philox4x32_10(U4{(unsigned)i, (unsigned)(step & 0xffffffffull), (unsigned)(step >> 32), 0x4C47u},
                          (unsigned)(seed & 0xffffffffull), (unsigned)(seed >> 32));
     double z0, z1, z2, z3;
@@ -128,6 +130,8 @@ __global__ void k_md_step(int n, double dt, double* __restrict__ x, double* __re
     if (dx * dx + dy * dy + dz * dz > half_skin2) *rebuild_flag = 1;
   }
 }
+
+__global__ void k_inc_counter(unsigned long long* c) { *c += 1ull; }
 
 __global__ void k_mark_rebuilt(int n, const double* __restrict__ x, double* __restrict__ x_ref, int* flag) {
   if (*flag == 0) return;
@@ -180,17 +184,24 @@ extern "C" int fennol_forces_finalize(const float* forces4, int natoms, float sc
 
 extern "C" int fennol_md_step(int natoms, double dt, double* x, double* v, const double* inv_mass,
                               const float* forces4, double force_scale, double a1, const double* a2,
-                              unsigned long long seed, unsigned long long step, float* coords,
-                              const int* species_idx, float* xyzs, const double* x_ref,
-                              double half_skin, int* rebuild_flag, void* stream) {
+                              unsigned long long seed, unsigned long long* step_counter,
+                              float* coords, const int* species_idx, float* xyzs,
+                              const double* x_ref, double half_skin, int* rebuild_flag,
+                              void* stream) {
   if (natoms < 0 || !(dt > 0)) return FENNOL_ERR_INVALID;
+  if (a2 && !step_counter) return FENNOL_ERR_INVALID;
   if (natoms == 0) return FENNOL_OK;
   if (!x || !v || !inv_mass || !forces4) return FENNOL_ERR_INVALID;
   if (xyzs && !species_idx) return FENNOL_ERR_INVALID;
-  k_md_step<<<(natoms + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
-      natoms, dt, x, v, inv_mass, (const float4*)forces4, force_scale, a1, a2, seed, step, coords,
-      species_idx, (float4*)xyzs, x_ref, half_skin * half_skin, rebuild_flag);
+  cudaStream_t st = (cudaStream_t)stream;
+  k_md_step<<<(natoms + 255) / 256, 256, 0, st>>>(
+      natoms, dt, x, v, inv_mass, (const float4*)forces4, force_scale, a1, a2, seed, step_counter,
+      coords, species_idx, (float4*)xyzs, x_ref, half_skin * half_skin, rebuild_flag);
   FNL_CHECK_LAUNCH();
+  if (step_counter) {
+    k_inc_counter<<<1, 1, 0, st>>>(step_counter);
+    FNL_CHECK_LAUNCH();
+  }
   return FENNOL_OK;
 }
 

@@ -32,6 +32,9 @@ ATOMIC_MASSES = {
 
 ANI2X_SPECIES = ("H", "C", "N", "O", "S", "F", "Cl")
 
+# Last-layer scale of the random model used by MD workloads (see init_weights).
+MD_OUTPUT_SCALE = 0.02
+
 
 @dataclasses.dataclass(frozen=True)
 class AEVConfig:
@@ -126,11 +129,15 @@ Weights = List[Dict[str, List[Tuple[np.ndarray, np.ndarray]]]]
 
 
 def init_weights(aev: AEVConfig, mlp: MLPConfig, seed: int = 0,
-                 n_models: int = 1, bias_std: float = 0.0) -> Weights:
+                 n_models: int = 1, bias_std: float = 0.0, output_scale: float = 1.0) -> Weights:
     """Seeded random weights: kernel ~ N(0, 1/fan_in), bias 0 (or N(0, bias_std)).
 
     Model ``m`` of an ensemble uses seed ``seed + 1000*m`` so that members are
-    independent.  Float64 master copy; device packing casts as needed.
+    independent.  ``output_scale`` multiplies the last layer's kernel: with
+    the unscaled N(0, 1/fan_in) network atomic energies vary by ~40 kcal/mol
+    and the random landscape pulls atoms together within ~10 fs of MD, so MD
+    workloads use a small scale (0.02) that keeps forces near thermal size.
+    Float64 master copy; device packing casts as needed.
     """
     dims = [aev.aev_length, *mlp.hidden, mlp.output_dim]
     out: Weights = []
@@ -141,6 +148,8 @@ def init_weights(aev: AEVConfig, mlp: MLPConfig, seed: int = 0,
             layers = []
             for din, dout in zip(dims[:-1], dims[1:]):
                 w = rng.standard_normal((din, dout)) / np.sqrt(din)
+                if dout == dims[-1] and din == dims[-2]:
+                    w = w * output_scale
                 if bias_std > 0:
                     b = rng.standard_normal(dout) * bias_std
                 else:

@@ -311,7 +311,7 @@ class ANIPotential:
     def __init__(self, aev: AEVConfig = AEVConfig(), mlp: MLPConfig = MLPConfig(),
                  weights: Optional[Weights] = None, precision: str = "fp32", device="cuda",
                  seed: int = 0, n_models: int = 1, energy_unit: str = "Ha",
-                 minimum_image: bool = True):
+                 minimum_image: bool = True, output_scale: float = 1.0):
         if precision not in _lib.PRECISIONS:
             raise ValueError(f"precision must be one of {list(_lib.PRECISIONS)}")
         _lib.load()
@@ -320,7 +320,7 @@ class ANIPotential:
             raise RuntimeError("ANIPotential runs on CUDA devices only")
         self.aev_cfg, self.mlp_cfg = aev, mlp
         if weights is None:
-            weights = init_weights(aev, mlp, seed=seed, n_models=n_models)
+            weights = init_weights(aev, mlp, seed=seed, n_models=n_models, output_scale=output_scale)
         self.weights = weights
         self.precision = _lib.PRECISIONS[precision]
         self.precision_name = precision
@@ -334,6 +334,7 @@ class ANIPotential:
         self._cache: Dict[tuple, tuple] = {}
         self.capacity_margin = 1.05
         self.add_neigh = 8
+        self._tc_launches = 6
 
     # ------------------------------------------------------------------ layout
     def layout(self, species, natoms, cells=None) -> BatchLayout:
@@ -350,6 +351,12 @@ class ANIPotential:
         g = GraphBuffers(layout, rc, skin, cap, cap_radial)
         ws = Workspace(self, layout)
         return g, ws
+
+    def mlp_launches(self) -> int:
+        """Kernels launched by one fennol_mlp_energy_grad call."""
+        if self.precision == _lib.MLP_FP32:
+            return 7 * self.mlp.n_models
+        return self._tc_launches
 
     # --------------------------------------------------------------- launches
     def launch_forces(self, layout: BatchLayout, g: GraphBuffers, ws: Workspace, stream: int,

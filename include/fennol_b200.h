@@ -270,14 +270,16 @@ int fennol_forces_finalize(const float* forces4, int natoms, float scale, float*
  * Units: A, ps, kcal/mol; inv_mass[i] = 1/m_i in the same system; forces4
  * holds -dE/dx in model units and is multiplied by force_scale.  xi are
  * standard normal numbers from a counter-based Philox4x32-10 stream keyed by
- * (seed, step).  Also writes float32 positions (coords) and packed xyzs for
- * the next force call, and sets *rebuild_flag = 1 when an atom moved more
- * than half the skin since the last rebuild (x_ref).  If rebuild_flag is
- * NULL no displacement check is done.
+ * (seed, *step_counter, atom); step_counter is a device uint64 that the call
+ * increments after the step, so a CUDA graph of the step draws new noise on
+ * every replay (required when a2 != NULL).  Also writes float32 positions
+ * (coords) and packed xyzs for the next force call, and sets
+ * *rebuild_flag = 1 when an atom moved more than half the skin since the
+ * last rebuild (x_ref).  If rebuild_flag is NULL no displacement check is done.
  */
 int fennol_md_step(int natoms, double dt, double* x, double* v, const double* inv_mass,
                    const float* forces4, double force_scale, double a1, const double* a2,
-                   unsigned long long seed, unsigned long long step, float* coords,
+                   unsigned long long seed, unsigned long long* step_counter, float* coords,
                    const int* species_idx, float* xyzs, const double* x_ref, double half_skin,
                    int* rebuild_flag, void* stream);
 
