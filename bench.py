@@ -113,7 +113,7 @@ def measured_peaks():
         return 6650.0, 1590.0, 1400.0, "fallback"
 
 
-def make_engine(workload, precision, device, seed=0):
+def make_engine(workload, precision, device, seed=0, bf16_weights=True):
     from fennol_b200.md import MDEngine
     from fennol_b200.potential import ANIPotential
     from fennol_b200.systems import water_box
@@ -123,7 +123,7 @@ def make_engine(workload, precision, device, seed=0):
     w = WORKLOADS[workload]
     box = water_box(w["n_side"], seed=seed)
     pot = ANIPotential(precision=precision, device=device, seed=0, n_models=w["n_models"],
-                       output_scale=MD_OUTPUT_SCALE)
+                       output_scale=MD_OUTPUT_SCALE, bf16_weights=bf16_weights)
     eng = MDEngine(pot, box.coordinates, box.species, box.cell, dt_fs=0.5, thermostat=w["thermostat"],
                    temperature=300.0, gamma_ps=1.0, skin=1.0, trigger="displacement", seed=seed)
     return box, pot, eng
@@ -300,7 +300,7 @@ def main():
     from fennol_b200 import _lib
     precision = args.precision
     if precision is None:
-        precision = "bf16x3" if os.environ.get("FENNOL_BENCH_FP32_ONLY") is None else "fp32"
+        precision = "bf16x2" if os.environ.get("FENNOL_BENCH_FP32_ONLY") is None else "fp32"
     w = WORKLOADS[args.workload]
     try:
         box, pot, eng = make_engine(args.workload, precision, device, seed=rank)
@@ -329,6 +329,7 @@ def main():
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "bf16" if precision.startswith("bf16") else "f32", "data": "synthetic",
            "config": {"workload": w["desc"], "atoms_per_gpu": box.natoms, "precision": precision,
+                      "weights": "BF16-representable (seeded N(0, 1/fan_in) rounded to BF16)",
                       "mlp_precision": {"fp32": "float32 CUDA cores",
                                         "bf16": "tcgen05 BF16, FP32 accumulate",
                                         "bf16x2": "tcgen05 BF16 hi+lo activations (2 MMAs)",
@@ -359,9 +360,11 @@ def main():
             res["speedup_vs_fp32_form"] = value / world / v32
             del eng32, pot32
         from fennol_b200.potential import ANIPotential
-        spec = ANIPotential(precision=precision, device=device, seed=0, n_models=w["n_models"])
+        spec = ANIPotential(precision=precision, device=device, seed=0, n_models=w["n_models"],
+                            bf16_weights=True)
         res["accuracy_vs_fp64_oracle"] = accuracy(spec, box)
-        res["accuracy_vs_fp64_oracle"]["model"] = "unscaled N(0, 1/fan_in) random-init weights"
+        res["accuracy_vs_fp64_oracle"]["model"] = ("unscaled N(0, 1/fan_in) random-init weights "
+                                                   "rounded to BF16 (same weights in the oracle)")
         del spec
         res["e2e"] = e2e(pot, box, max(5, args.steps // 3), 3)
         if not args.no_cpu_baseline:

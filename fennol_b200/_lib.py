@@ -83,7 +83,8 @@ _SIGNATURES = {
     "fennol_aev_backward": (I, [P, I, P, P, P, P, P, I, C.POINTER(AEVParams), P, P, I, P, P, P]),
     "fennol_mlp_workspace_bytes": (SZ, [I, I, I, C.POINTER(MLPWeights)]),
     "fennol_mlp_energy_grad": (I, [I, I, I, P, P, C.POINTER(MLPWeights), P, P, P, P, P, SZ, P]),
-    "fennol_energy_reduce": (I, [P, P, I, P, I, D, P, P, P]),
+    "fennol_energy_workspace_bytes": (SZ, [I, I]),
+    "fennol_energy_reduce": (I, [P, P, I, P, I, D, P, P, P, SZ, P]),
     "fennol_forces_finalize": (I, [P, I, F, P, P]),
     "fennol_md_step": (I, [I, D, P, P, P, P, D, D, P, ULL, P, P, P, P, P, D, P, P]),
     "fennol_md_mark_rebuilt": (I, [I, P, P, P, P]),

@@ -14,25 +14,93 @@ using namespace fnl;
 
 namespace {
 
-__global__ void k_energy_reduce(const float* __restrict__ e_rows, const int* __restrict__ atom_row,
-                                const int* __restrict__ sys_start, double scale,
-                                double* __restrict__ energy, double* __restrict__ e_atom) {
+// Two-level fixed-order reduction: every block sums a contiguous chunk of
+// one system's atoms into partial[b*chunks + c]; one warp per system then
+// adds the partials in order.  Deterministic for a given batch layout.
+constexpr int kRedChunk = 1024;
+
+__global__ void k_energy_partial(const float* __restrict__ e_rows, const int* __restrict__ atom_row,
+                                 const int* __restrict__ sys_start, const int* __restrict__ chunk_off,
+                                 int nsys, double scale, double* __restrict__ partial,
+                                 double* __restrict__ e_atom) {
   __shared__ double part[256];
-  int b = blockIdx.x;
-  int i0 = sys_start[b], i1 = sys_start[b + 1];
-  double s = 0.0;
-  for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
-    double e = scale * (double)e_rows[atom_row[i]];
-    if (e_atom) e_atom[i] = e;
-    s += e;
-  }
-  part[threadIdx.x] = s;
-  __syncthreads();
-  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-    if ((int)threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
+  const int total = chunk_off[nsys];
+  for (int w = blockIdx.x; w < total; w += gridDim.x) {
+    // system b with chunk_off[b] <= w < chunk_off[b+1] (binary search)
+    int lo = 0, hi = nsys - 1;
+    while (lo < hi) {
+      int mid = (lo + hi + 1) >> 1;
+      if (chunk_off[mid] <= w) lo = mid; else hi = mid - 1;
+    }
+    const int b = lo, c = w - chunk_off[b];
+    const int i0 = sys_start[b] + c * kRedChunk;
+    const int i1 = min(i0 + kRedChunk, sys_start[b + 1]);
+    double s = 0.0;
+    for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+      double e = scale * (double)e_rows[atom_row[i]];
+      if (e_atom) e_atom[i] = e;
+      s += e;
+    }
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+      if ((int)threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[w] = part[0];
     __syncthreads();
   }
-  if (threadIdx.x == 0) energy[b] = part[0];
+}
+
+__global__ void k_energy_final(const int* __restrict__ chunk_off, int nsys, const double* __restrict__ partial,
+                               double* __restrict__ energy) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nsys) return;
+  double s = 0.0;
+  for (int k = chunk_off[b]; k < chunk_off[b + 1]; ++k) s += partial[k];
+  energy[b] = s;
+}
+
+// chunk_off[b] = sum_{b' < b} max(1, ceil(n_b' / kRedChunk)) (one block, tiled scan).
+__global__ void k_chunk_offsets(const int* __restrict__ sys_start, int nsys, int* __restrict__ chunk_off) {
+  __shared__ int warp_sums[32];
+  __shared__ int carry;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if (tid == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < nsys; base += blockDim.x) {
+    int b = base + tid;
+    int v = 0;
+    if (b < nsys) {
+      int n = sys_start[b + 1] - sys_start[b];
+      v = max(1, (n + kRedChunk - 1) / kRedChunk);
+    }
+    int incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) warp_sums[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+      int nw = blockDim.x >> 5;
+      int s = lane < nw ? warp_sums[lane] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, s, o);
+        if (lane >= o) s += t;
+      }
+      if (lane < nw) warp_sums[lane] = s;
+    }
+    __syncthreads();
+    int excl = carry + (wid > 0 ? warp_sums[wid - 1] : 0) + incl - v;
+    if (b < nsys) chunk_off[b] = excl;
+    __syncthreads();
+    if (tid == blockDim.x - 1) carry = excl + v;
+    __syncthreads();
+  }
+  if (tid == 0) chunk_off[nsys] = carry;
 }
 
 __global__ void k_forces_finalize(const float4* __restrict__ f4, int n, float scale, float* __restrict__ f) {
@@ -159,14 +227,31 @@ __global__ void k_kinetic(int n, const double* __restrict__ v, const double* __r
 
 }  // namespace
 
+extern "C" size_t fennol_energy_workspace_bytes(int natoms, int nsys) {
+  if (natoms < 0 || nsys < 0) return 0;
+  size_t chunks = (size_t)natoms / kRedChunk + (size_t)nsys + 1;
+  return 256 + (size_t)(nsys + 1) * sizeof(int) + 256 + chunks * sizeof(double);
+}
+
 extern "C" int fennol_energy_reduce(const float* e_rows, const int* atom_row, int natoms,
                                     const int* sys_start, int nsys, double scale, double* energy,
-                                    double* e_atom, void* stream) {
+                                    double* e_atom, void* workspace, size_t workspace_bytes,
+                                    void* stream) {
   if (natoms < 0 || nsys < 0) return FENNOL_ERR_INVALID;
   if (nsys == 0) return FENNOL_OK;
-  if (!e_rows || !atom_row || !sys_start || !energy) return FENNOL_ERR_INVALID;
-  k_energy_reduce<<<nsys, 256, 0, (cudaStream_t)stream>>>(e_rows, atom_row, sys_start, scale, energy,
-                                                          e_atom);
+  if (!e_rows || !atom_row || !sys_start || !energy || !workspace) return FENNOL_ERR_INVALID;
+  if (workspace_bytes < fennol_energy_workspace_bytes(natoms, nsys)) return FENNOL_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  int* chunk_off = (int*)workspace;
+  double* partial = (double*)((char*)workspace + ((sizeof(int) * (size_t)(nsys + 1) + 255) / 256 * 256));
+  k_chunk_offsets<<<1, 1024, 0, st>>>(sys_start, nsys, chunk_off);
+  FNL_CHECK_LAUNCH();
+  int blocks = natoms / kRedChunk + nsys;
+  if (blocks > 4 * 148) blocks = 4 * 148;
+  k_energy_partial<<<blocks, 256, 0, st>>>(e_rows, atom_row, sys_start, chunk_off, nsys, scale, partial,
+                                           e_atom);
+  FNL_CHECK_LAUNCH();
+  k_energy_final<<<(nsys + 127) / 128, 128, 0, st>>>(chunk_off, nsys, partial, energy);
   FNL_CHECK_LAUNCH();
   return FENNOL_OK;
 }

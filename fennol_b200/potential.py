@@ -296,6 +296,8 @@ class Workspace:
         self.forces = torch.zeros((n, 3), dtype=torch.float32, device=dev)
         self.energy = torch.zeros(layout.nsys, dtype=torch.float64, device=dev)
         self.e_atom = torch.zeros(n, dtype=torch.float64, device=dev)
+        ews = _lib.load().fennol_energy_workspace_bytes(layout.n, layout.nsys)
+        self.energy_ws = torch.zeros(int(ews), dtype=torch.uint8, device=dev)
         self.status = torch.zeros(_lib.STATUS_WORDS, dtype=torch.int32, device=dev)
 
 
@@ -304,6 +306,8 @@ class ANIPotential:
 
     ``precision``: ``"fp32"`` (CUDA-core GEMMs), ``"bf16"``, ``"bf16x2"`` or
     ``"bf16x3"`` (tcgen05 tensor-core GEMMs with 1, 2 or 3 BF16 products).
+    ``bf16_weights`` rounds the kernels to BFloat16 (a model stored in BF16);
+    bf16x2 is exact in the weights for such a model.
     Energies are returned in Hartree (FeNNol's default model unit) and
     forces in Hartree/Angstrom, unless ``energy_unit="kcalpermol"``.
     """
@@ -311,7 +315,8 @@ class ANIPotential:
     def __init__(self, aev: AEVConfig = AEVConfig(), mlp: MLPConfig = MLPConfig(),
                  weights: Optional[Weights] = None, precision: str = "fp32", device="cuda",
                  seed: int = 0, n_models: int = 1, energy_unit: str = "Ha",
-                 minimum_image: bool = True, output_scale: float = 1.0):
+                 minimum_image: bool = True, output_scale: float = 1.0,
+                 bf16_weights: bool = False):
         if precision not in _lib.PRECISIONS:
             raise ValueError(f"precision must be one of {list(_lib.PRECISIONS)}")
         _lib.load()
@@ -321,6 +326,8 @@ class ANIPotential:
         self.aev_cfg, self.mlp_cfg = aev, mlp
         if weights is None:
             weights = init_weights(aev, mlp, seed=seed, n_models=n_models, output_scale=output_scale)
+        if bf16_weights:
+            weights = round_weights_bf16(weights)
         self.weights = weights
         self.precision = _lib.PRECISIONS[precision]
         self.precision_name = precision
@@ -374,7 +381,7 @@ class ANIPotential:
              ws.mlp_ws.data_ptr(), ws.mlp_ws.numel(), stream)
         call("fennol_energy_reduce", ws.e_rows.data_ptr(), layout.t_atom_row.data_ptr(), n,
              layout.t_sys_start.data_ptr(), layout.nsys, float(self.unit_scale), ws.energy.data_ptr(),
-             ws.e_atom.data_ptr(), stream)
+             ws.e_atom.data_ptr(), ws.energy_ws.data_ptr(), ws.energy_ws.numel(), stream)
         if want_forces:
             ws.forces4.zero_()
             call("fennol_aev_backward", ws.xyzs.data_ptr(), n, layout.t_atom_sys.data_ptr(),

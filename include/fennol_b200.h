@@ -245,15 +245,19 @@ int fennol_mlp_energy_grad(int precision, int rows, int ntiles, const int* tile_
 /* Reductions and outputs                                                    */
 /* ------------------------------------------------------------------------ */
 
+/* Workspace of fennol_energy_reduce, in bytes. */
+size_t fennol_energy_workspace_bytes(int natoms, int nsys);
+
 /*
  * Per-system energies in float64: energy[b] = scale * sum_{i in b}
- * e_rows[atom_row[i]] (fixed summation order).  Replaces the segment_sum of
- * FENNIX.total_energy (fennix.py:218-258).  e_atom (float64 [natoms], may be
- * NULL) receives scale * per-atom energies in input order.
+ * e_rows[atom_row[i]] (fixed summation order: 1024-atom chunks, then the
+ * chunk sums in order).  Replaces the segment_sum of FENNIX.total_energy
+ * (fennix.py:218-258).  e_atom (float64 [natoms], may be NULL) receives
+ * scale * per-atom energies in input order.
  */
 int fennol_energy_reduce(const float* e_rows, const int* atom_row, int natoms,
                          const int* sys_start, int nsys, double scale, double* energy,
-                         double* e_atom, void* stream);
+                         double* e_atom, void* workspace, size_t workspace_bytes, void* stream);
 
 /* forces[i*3+k] = scale * forces4[i*4+k] (float32 output). */
 int fennol_forces_finalize(const float* forces4, int natoms, float scale, float* forces,
