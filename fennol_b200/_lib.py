@@ -22,6 +22,7 @@ ERR_INVALID = -1
 ERR_CUDA = -2
 ERR_UNSUPPORTED = -3
 ERR_WORKSPACE = -4
+ERR_STATIC_LIMIT = -5
 
 STATUS_WORDS = 8
 ST_NBR_OVERFLOW, ST_NBR_MAXCOUNT, ST_FILTER_OVERFLOW, ST_FILTER_MAXCOUNT = 0, 1, 2, 3
@@ -35,7 +36,8 @@ MLP_FP32, MLP_BF16, MLP_BF16X2, MLP_BF16X3 = 0, 1, 2, 3
 PRECISIONS = {"fp32": MLP_FP32, "bf16": MLP_BF16, "bf16x2": MLP_BF16X2, "bf16x3": MLP_BF16X3}
 
 _ERRNAMES = {ERR_INVALID: "invalid argument", ERR_CUDA: "CUDA launch failure",
-             ERR_UNSUPPORTED: "unsupported parameters", ERR_WORKSPACE: "workspace too small"}
+             ERR_UNSUPPORTED: "unsupported parameters", ERR_WORKSPACE: "workspace too small",
+             ERR_STATIC_LIMIT: "input larger than the fixed in-library scratch"}
 
 
 class LibraryError(RuntimeError):
@@ -76,6 +78,8 @@ _SIGNATURES = {
     "fennol_graph_plan": (I, [I, P, P, D, P, P]),
     "fennol_graph_workspace_bytes": (SZ, [I, I]),
     "fennol_graph_build": (I, [P, I, P, I, P, P, P, P, P, P, I, D, I, P, P, P, P, P, SZ, P, P]),
+    "fennol_graph_build_noalloc": (I, [P, I, P, I, P, P, P, P, P, P, I, D, I, P, P, P, P, P, P]),
+    "fennol_graph_noalloc_limits": (I, [P, P, P]),
     "fennol_graph_filter": (I, [P, I, P, P, P, P, P, I, D, I, P, P, P, P, P]),
     "fennol_aev_length": (I, [C.POINTER(AEVParams)]),
     "fennol_pack_atoms": (I, [P, P, I, P, P]),

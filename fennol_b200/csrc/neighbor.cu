@@ -547,3 +547,78 @@ extern "C" int fennol_graph_filter(const float* coords, int natoms, const int* a
   FNL_CHECK_LAUNCH();
   return FENNOL_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of fennol_graph_build.
+//
+// Callers that cannot allocate device memory -- an XLA FFI handler, where the
+// framework owns every buffer and a call must not create memory behind the
+// allocator's back, or a stream being captured into a CUDA graph, where
+// cudaMalloc is not allowed -- use this entry point.  Its cell-list scratch
+// is a file-scope __device__ array sized for at most kStaticMaxAtoms atoms and
+// kStaticMaxCells cells; every GPU that loads the library holds that array
+// (about 2.2 MB) until the process exits.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace {
+
+constexpr int kStaticMaxAtoms = 65536;
+constexpr int kStaticMaxCells = 32768;
+constexpr int kStaticMaxDevices = 64;
+
+constexpr size_t round256(size_t v) { return (v + 255) / 256 * 256; }
+// Same carve-up as ws_layout(): counts, starts, cursor, cell_atoms, atom_cell, pos, at.
+constexpr size_t static_scratch_bytes(size_t n, size_t c) {
+  return round256(4 * c) + round256(4 * (c + 1)) + round256(4 * c) + round256(4 * n) + round256(4 * n) +
+         round256(16 * n) + round256(4 * n);
+}
+constexpr size_t kStaticScratchBytes = static_scratch_bytes(kStaticMaxAtoms, kStaticMaxCells);
+
+static __device__ __align__(256) unsigned char g_graph_scratch[kStaticScratchBytes];
+
+std::mutex g_scratch_mu;
+void* g_scratch_addr[kStaticMaxDevices] = {};
+
+// Device address of g_graph_scratch on the current device, looked up once
+// per device.  In host code the symbol itself is only a host-side stand-in.
+int scratch_address(void** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kStaticMaxDevices) return FENNOL_ERR_CUDA;
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  if (!g_scratch_addr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_graph_scratch) != cudaSuccess || !p) return FENNOL_ERR_CUDA;
+    g_scratch_addr[dev] = p;
+  }
+  *out = g_scratch_addr[dev];
+  return FENNOL_OK;
+}
+
+}  // namespace
+
+extern "C" int fennol_graph_build_noalloc(const float* coords, int natoms, const int* atom_sys, int nsys,
+                                          const int* sys_start, const int* sys_mode, const float* sys_cell,
+                                          const float* sys_recip, const int* sys_grid, const int* sys_nrep,
+                                          int ncells_total, double cutoff, int capacity, int* nbr_j,
+                                          unsigned* nbr_shift, int* nbr_count, int* status,
+                                          const int* enable_flag, void* stream) {
+  if (natoms > kStaticMaxAtoms || ncells_total > kStaticMaxCells) return FENNOL_ERR_STATIC_LIMIT;
+  if (natoms < 0 || ncells_total < 0) return FENNOL_ERR_INVALID;
+  if (fennol_graph_workspace_bytes(natoms, ncells_total) > kStaticScratchBytes) return FENNOL_ERR_STATIC_LIMIT;
+  void* scratch = nullptr;
+  int rc = scratch_address(&scratch);
+  if (rc != FENNOL_OK) return rc;
+  // fennol_graph_build clears the cell histogram it needs before use; the
+  // rest of the scratch is fully rewritten by each call.
+  return fennol_graph_build(coords, natoms, atom_sys, nsys, sys_start, sys_mode, sys_cell, sys_recip,
+                            sys_grid, sys_nrep, ncells_total, cutoff, capacity, nbr_j, nbr_shift, nbr_count,
+                            status, scratch, kStaticScratchBytes, enable_flag, stream);
+}
+
+extern "C" int fennol_graph_noalloc_limits(int* max_atoms, int* max_cells, size_t* scratch_bytes) {
+  if (max_atoms) *max_atoms = kStaticMaxAtoms;
+  if (max_cells) *max_cells = kStaticMaxCells;
+  if (scratch_bytes) *scratch_bytes = kStaticScratchBytes;
+  return FENNOL_OK;
+}

@@ -34,6 +34,7 @@ extern "C" {
 #define FENNOL_ERR_CUDA (-2)
 #define FENNOL_ERR_UNSUPPORTED (-3)
 #define FENNOL_ERR_WORKSPACE (-4)
+#define FENNOL_ERR_STATIC_LIMIT (-5) /* input larger than a fixed in-library scratch */
 
 #define FENNOL_STATUS_WORDS 8
 #define FENNOL_ST_NBR_OVERFLOW 0
@@ -107,6 +108,32 @@ int fennol_graph_build(const float* coords, int natoms, const int* atom_sys, int
                        int ncells_total, double cutoff, int capacity, int* nbr_j,
                        unsigned* nbr_shift, int* nbr_count, int* status, void* workspace,
                        size_t workspace_bytes, const int* enable_flag, void* stream);
+
+/*
+ * Allocation-free variant of fennol_graph_build (no counterpart in the
+ * reference).  For callers that cannot allocate device memory: an XLA FFI
+ * handler, where the framework owns every buffer, or a stream under CUDA
+ * graph capture, where cudaMalloc is not allowed.  Same arguments and
+ * results as fennol_graph_build, but the cell-list scratch is a fixed array
+ * inside the library (one per GPU, about 2.2 MB, held until the process
+ * exits) instead of a caller workspace; the caller still passes inputs and
+ * outputs.  Limits: natoms <= 65536 and ncells_total <= 32768, otherwise
+ * FENNOL_ERR_STATIC_LIMIT and nothing is launched (see
+ * fennol_graph_noalloc_limits).  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  All calls share the one array: calls whose
+ * work overlaps on the GPU (two streams, or two threads) race on it and must
+ * be serialised by the caller.  Allocates nothing.
+ */
+int fennol_graph_build_noalloc(const float* coords, int natoms, const int* atom_sys, int nsys,
+                               const int* sys_start, const int* sys_mode, const float* sys_cell,
+                               const float* sys_recip, const int* sys_grid, const int* sys_nrep,
+                               int ncells_total, double cutoff, int capacity, int* nbr_j,
+                               unsigned* nbr_shift, int* nbr_count, int* status,
+                               const int* enable_flag, void* stream);
+
+/* Limits and scratch size of fennol_graph_build_noalloc (host only). */
+int fennol_graph_noalloc_limits(int* max_atoms, int* max_cells, size_t* scratch_bytes);
 
 /*
  * Re-filter a neighbour list to a smaller cutoff from current positions.
