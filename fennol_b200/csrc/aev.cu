@@ -22,7 +22,7 @@ using namespace fnl;
 
 namespace {
 
-constexpr int kAevWarps = 4;
+constexpr int kAevWarps = 8;
 constexpr int kMaxS = 8;
 constexpr int kMaxP = kMaxS * (kMaxS + 1) / 2;
 constexpr int kCapA = FENNOL_MAX_ANGULAR_NEIGHBORS;
@@ -33,6 +33,10 @@ struct AevConst {
   float rc, rca, rc2, rca2;   // cutoffs and float32 thresholds
   float pi_rc, pi_rca;        // pi / cutoff
   float eta_r, eta_a, zeta, c_ang;  // c_ang = 2^(1-zeta)
+  int zeta_n;                       // floor(zeta) and zeta - floor(zeta)
+  float zeta_f;
+  int zeta1_n;                      // the same split of zeta - 1
+  float zeta1_f;
   float shift_r[32];
   float shift_a[32];
   float cosz[32], sinz[32];
@@ -62,6 +66,15 @@ bool make_const(const fennol_aev_params* p, AevConst* k) {
   k->eta_a = p->angular_eta;
   k->zeta = p->zeta;
   k->c_ang = (float)std::pow(2.0, 1.0 - (double)p->zeta);
+  {
+    double zn = std::floor((double)p->zeta);
+    k->zeta_n = (int)zn;
+    k->zeta_f = (float)((double)p->zeta - zn);
+    double z1 = std::floor((double)p->zeta - 1.0);
+    k->zeta1_n = (int)z1;
+    k->zeta1_f = (float)((double)p->zeta - 1.0 - z1);
+    if (p->zeta < 1.0f || p->zeta > 64.0f) return false;
+  }
   for (int r = 0; r < 32; ++r) {
     k->shift_r[r] = r < RD ? (float)(p->radial_start + (p->radial_cutoff - p->radial_start) * r / RD) : 0.f;
     k->shift_a[r] = r < AD ? (float)(p->angular_start + (p->angular_cutoff - p->angular_start) * r / AD) : 0.f;
@@ -70,15 +83,6 @@ bool make_const(const fennol_aev_params* p, AevConst* k) {
     k->sinz[r] = r < AS ? (float)std::sin(z) : 0.f;
   }
   return true;
-}
-
-// Triplet index t -> (a, b) with a < b, enumerated b = 1.., a = 0..b-1.
-__device__ __forceinline__ void triplet_ab(int t, int& a, int& b) {
-  int bb = (int)((1.0f + sqrtf(1.0f + 8.0f * (float)t)) * 0.5f);
-  while (bb * (bb - 1) / 2 > t) --bb;
-  while ((bb + 1) * bb / 2 <= t) ++bb;
-  b = bb;
-  a = t - bb * (bb - 1) / 2;
 }
 
 __device__ __forceinline__ void load_cell(const float* sys_cell, int b, float* c) {
@@ -106,19 +110,206 @@ __device__ __forceinline__ void edge_vec(float4 pi, float4 pj, unsigned sh, cons
 
 __device__ __forceinline__ __nv_bfloat16 to_bf16(float x) { return __float2bfloat16_rn(x); }
 
-// Shared-memory carve-up per warp (floats).
-struct FwdSmem {
-  float* rad;    // [S][32]
-  float* ang;    // [P][32]
-  float* au;     // [kCapA][4] ux,uy,uz,d
-  float* afc;    // [kCapA]
-  int* asp;      // [kCapA]
-  float* stA;    // [32][33] angular factors (scaled by the switch product)
-  float* stB;    // [32][33] radial factors
-  int* stP;      // [32]
+// ------------------------------------------------------------------------------
+// Species-sorted staging shared by the forward and adjoint kernels.
+//
+// The warp streams the atom's radial row once, computes the edge geometry with
+// the reference's float32 arithmetic and writes it unsorted to `tmp`; a
+// ballot-based counting sort then places the radial neighbours (d, 0.25 fc)
+// and the angular ones (unit vector, d, fc, slot) grouped by species, so
+// every species block and every species-pair block of triplets is contiguous.
+// ------------------------------------------------------------------------------
+struct Stage {
+  float4* tmp;   // [cap] (vx, vy, vz, d2) unsorted
+  int* tkey;     // [cap] species | angular<<8
+  float2* rd;    // [cap] radial (d, 0.25*fc) sorted by species
+  float4* au;    // [kCapA] angular (ux, uy, uz, d) sorted by species
+  float2* af;    // [kCapA] angular (fc, dfc)
+  int* aslot;    // [kCapA] radial row position of each angular neighbour
+  int* cntw;     // [32] per-species counters
 };
-__host__ __device__ __forceinline__ int fwd_smem_floats(int S, int P) {
-  return S * 32 + P * 32 + kCapA * 6 + 32 * 33 + 32 * 33 + 32;
+
+__host__ __device__ __forceinline__ size_t stage_bytes(int cap) {
+  // rounded to 16 bytes so that every per-warp carve-up keeps float4 alignment
+  return ((size_t)cap * (16 + 4 + 8) + (size_t)kCapA * (16 + 8 + 4) + 32 * 4 + 15) / 16 * 16;
+}
+
+__device__ __forceinline__ Stage carve_stage(char* base, int cap) {
+  Stage st;
+  st.tmp = (float4*)base;
+  st.au = (float4*)(base + (size_t)cap * 16);
+  st.rd = (float2*)(base + (size_t)cap * 16 + (size_t)kCapA * 16);
+  st.af = (float2*)((char*)st.rd + (size_t)cap * 8);
+  st.tkey = (int*)((char*)st.af + (size_t)kCapA * 8);
+  st.aslot = st.tkey + cap;
+  st.cntw = st.aslot + kCapA;
+  return st;
+}
+
+// Gaussian terms use the accurate expf: their arguments reach -50 and the
+// SFU-only __expf loses ~|x|*2^-24 of relative accuracy there.
+__device__ __forceinline__ float fexp(float x) { return expf(x); }
+__device__ __forceinline__ float exp2f_approx_pos(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// x^zeta for x >= 0 as x^n * x^f with n = floor(zeta): the integer power by
+// repeated squaring (a few roundings) and only the fractional power through
+// the SFU exp2/log2 approximations, whose log2 error is then scaled by f < 1
+// instead of by zeta (14.1).
+__device__ __forceinline__ float zeta_pow(float x, int n, float f) {
+  if (x <= 0.f) return 0.f;
+  float r = 1.f, b = x;
+  for (int e = n; e > 0; e >>= 1) {
+    if (e & 1) r *= b;
+    b *= b;
+  }
+  return f != 0.f ? r * exp2f_approx_pos(f * __log2f(x)) : r;
+}
+
+// Warp-collective: stage row i.  Returns, in lanes s < S, the per-species
+// radial and angular counts and exclusive offsets.  Lanes holding the same
+// species are grouped with __match_any_sync; per-warp counters live in `cntw`.
+template <bool kGrad>
+__device__ __forceinline__ void stage_row(const Stage& st, int* cntw, const float4* __restrict__ xyzs, float4 pi,
+                                          const float* c, const int* __restrict__ nbr_j,
+                                          const unsigned* __restrict__ nbr_shift, size_t row, int cnt,
+                                          const AevConst& K, int lane, int& cnt_r, int& off_r, int& cnt_a,
+                                          int& off_a, int& na_total) {
+  const int S = K.S;
+  // cntw[0..S): radial counts, [S..2S): angular counts, [2S..4S): running offsets
+  if (lane < 4 * S) cntw[lane] = 0;
+  __syncwarp();
+  const unsigned lt = (1u << lane) - 1u;
+  for (int k0 = 0; k0 < cnt; k0 += 32) {
+    const int k = k0 + lane;
+    int key = -1;
+    if (k < cnt) {
+      int j = __ldg(nbr_j + row + k);
+      unsigned sh = __ldg(nbr_shift + row + k);
+      float4 pj = xyzs[j];
+      float vx, vy, vz;
+      edge_vec(pi, pj, sh, c, vx, vy, vz);
+      float d2 = dist2_exact(vx, vy, vz);
+      int sj = __float_as_int(pj.w);
+      key = sj | ((d2 < K.rca2) << 8);
+      st.tmp[k] = make_float4(vx, vy, vz, d2);
+      st.tkey[k] = key;
+    }
+    const unsigned grp = __match_any_sync(0xffffffffu, key);
+    if (key >= 0 && (grp & lt) == 0) {  // group leader (two groups may share a species)
+      const int sj = key & 0xFF;
+      if (key >> 8) atomicAdd(cntw + S + sj, __popc(grp));
+      atomicAdd(cntw + sj, __popc(grp));
+    }
+    __syncwarp();
+  }
+  // the angular key groups also counted towards radial above; radial counts are
+  // per species regardless of the angular bit
+  int cr = lane < S ? cntw[lane] : 0;
+  int ca = lane < S ? cntw[S + lane] : 0;
+  int ir = cr, ia = ca;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int t1 = __shfl_up_sync(0xffffffffu, ir, o);
+    int t2 = __shfl_up_sync(0xffffffffu, ia, o);
+    if (lane >= o) {
+      ir += t1;
+      ia += t2;
+    }
+  }
+  cnt_r = cr;
+  cnt_a = ca;
+  off_r = ir - cr;
+  off_a = ia - ca;
+  na_total = __shfl_sync(0xffffffffu, ia, S - 1);
+  if (lane < S) {
+    cntw[2 * S + lane] = off_r;
+    cntw[3 * S + lane] = off_a;
+  }
+  __syncwarp();
+  for (int k0 = 0; k0 < cnt; k0 += 32) {
+    const int k = k0 + lane;
+    const int key = k < cnt ? st.tkey[k] : -1;
+    const int sj = key & 0xFF;
+    const int isang = key >= 0 ? (key >> 8) : 0;
+    // radial position: group by species only
+    const unsigned gr_ = __match_any_sync(0xffffffffu, key < 0 ? -1 : sj);
+    const unsigned ga_ = __match_any_sync(0xffffffffu, isang ? sj : -1);
+    int pos_r = 0, pos_a = -1;
+    if (key >= 0) pos_r = cntw[2 * S + sj] + __popc(gr_ & lt);
+    if (isang) pos_a = cntw[3 * S + sj] + __popc(ga_ & lt);
+    __syncwarp();
+    if (key >= 0 && (gr_ & lt) == 0) cntw[2 * S + sj] += __popc(gr_);
+    if (isang && (ga_ & lt) == 0) cntw[3 * S + sj] += __popc(ga_);
+    __syncwarp();
+    if (k < cnt) {
+      float4 v = st.tmp[k];
+      float d = sqrtf(fmaxf(v.w, 1e-5f));
+      float fc = d < K.rc ? 0.5f * cosf(d * K.pi_rc) + 0.5f : 0.f;
+      st.rd[pos_r] = make_float2(d, 0.25f * fc);
+      if (pos_a >= 0 && pos_a < kCapA) {
+        float inv = 1.0f / fmaxf(d, 1e-5f);
+        st.au[pos_a] = make_float4(v.x * inv, v.y * inv, v.z * inv, d);
+        float sa, ca2;
+        sincosf(d * K.pi_rca, &sa, &ca2);
+        float fca = d < K.rca ? 0.5f * ca2 + 0.5f : 0.f;
+        float dfca = d < K.rca ? -0.5f * K.pi_rca * sa : 0.f;
+        st.af[pos_a] = make_float2(fca, dfca);
+        if (kGrad) st.aslot[pos_a] = k;
+      }
+    }
+  }
+  __syncwarp();
+}
+
+// Triangular index t -> (a, b), 0 <= a < b < n, b-major.
+__device__ __forceinline__ void tri_ab(int t, int& a, int& b) {
+  int bb = (int)((1.0f + sqrtf(1.0f + 8.0f * (float)t)) * 0.5f);
+  while (bb * (bb - 1) / 2 > t) --bb;
+  while ((bb + 1) * bb / 2 <= t) ++bb;
+  b = bb;
+  a = t - bb * (bb - 1) / 2;
+}
+
+// Diagonal order of the pairs a < b of n items: d = b - a = 1, 2, ...; inside a
+// diagonal a increases.  Consecutive t rarely share an item (atomics stay
+// nearly conflict-free).
+__device__ __forceinline__ void diag_ab(int t, int n, int& a, int& b) {
+  float q = (float)(2 * n - 1);
+  int u = (int)((q - sqrtf(fmaxf(q * q - 8.0f * (float)t, 0.f))) * 0.5f);
+  auto start = [&](int uu) { return (uu * (2 * n - 1) - uu * uu) / 2; };
+  while (u > 0 && start(u) > t) --u;
+  while (start(u + 1) <= t) ++u;
+  a = t - start(u);
+  b = a + u + 1;
+}
+
+// Reduce v[32] over the warp so that lane f returns sum over lanes of v[f].
+__device__ __forceinline__ float transpose_reduce32(float* v, int lane) {
+#pragma unroll
+  for (int w = 16; w >= 1; w >>= 1) {
+    const bool upper = (lane & w) != 0;
+#pragma unroll
+    for (int k = 0; k < w; ++k) {
+      float send = upper ? v[k] : v[k + w];
+      float keep = upper ? v[k + w] : v[k];
+      v[k] = keep + __shfl_xor_sync(0xffffffffu, send, w);
+    }
+  }
+  return v[0];
+}
+
+__device__ __forceinline__ void store_feature(int out_kind, void* out, void* out_lo, size_t idx, float v) {
+  if (out_kind == FENNOL_AEV_F32) {
+    ((float*)out)[idx] = v;
+  } else {
+    __nv_bfloat16 hi = to_bf16(v);
+    ((__nv_bfloat16*)out)[idx] = hi;
+    if (out_kind == FENNOL_AEV_BF16X2) ((__nv_bfloat16*)out_lo)[idx] = to_bf16(v - __bfloat162float(hi));
+  }
 }
 
 template <int RD, int AD, int AS>
@@ -128,146 +319,101 @@ k_aev_forward(const float4* __restrict__ xyzs, int n, const int* __restrict__ at
               const unsigned* __restrict__ nbr_shift, const int* __restrict__ nbr_count, int cap,
               const AevConst K, const int* __restrict__ atom_row, int out_kind, void* __restrict__ out,
               void* __restrict__ out_lo, int ld, int* status) {
-  extern __shared__ float smem[];
+  extern __shared__ __align__(16) char smem_c[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int i = blockIdx.x * kAevWarps + warp;
   if (i >= n) return;
-  const int S = K.S, P = K.P;
-  float* base = smem + (size_t)warp * fwd_smem_floats(S, P);
-  FwdSmem sm;
-  sm.rad = base;
-  sm.ang = sm.rad + S * 32;
-  sm.au = sm.ang + P * 32;
-  sm.afc = sm.au + kCapA * 4;
-  sm.asp = (int*)(sm.afc + kCapA);
-  sm.stA = (float*)(sm.asp + kCapA);
-  sm.stB = sm.stA + 32 * 33;
-  sm.stP = (int*)(sm.stB + 32 * 33);
-
-  for (int k = lane; k < (S + P) * 32; k += 32) sm.rad[k] = 0.f;
-  __syncwarp();
-
+  const int S = K.S;
+  Stage st = carve_stage(smem_c + (size_t)warp * stage_bytes(cap), cap);
   const float4 pi = xyzs[i];
   float c[9];
   load_cell(sys_cell, atom_sys[i], c);
   int cnt = nbr_count[i];
   if (cnt > cap) cnt = cap;
-  const size_t row = (size_t)i * cap;
-  constexpr int nh = 32 / RD;    // neighbours per radial step
-  const int r_lane = lane % RD, h_lane = lane / RD;
-  const float eta_r = K.eta_r, sr = K.shift_r[r_lane];
-  int na = 0;
-
-  // ---- radial terms + angular neighbour staging --------------------------------
-  for (int k0 = 0; k0 < cnt; k0 += 32) {
-    int k = k0 + lane;
-    float d = 0.f, fc = 0.f;
-    int sj = -1;
-    bool is_ang = false;
-    float vx = 0.f, vy = 0.f, vz = 0.f;
-    if (k < cnt) {
-      int j = __ldg(nbr_j + row + k);
-      unsigned sh = __ldg(nbr_shift + row + k);
-      float4 pj = xyzs[j];
-      edge_vec(pi, pj, sh, c, vx, vy, vz);
-      float d2 = dist2_exact(vx, vy, vz);
-      d = sqrtf(fmaxf(d2, 1e-5f));
-      fc = d < K.rc ? 0.5f * cosf(d * K.pi_rc) + 0.5f : 0.f;
-      sj = __float_as_int(pj.w);
-      is_ang = d2 < K.rca2;
-    }
-    // stage radial data (d, 0.25*fc, species) in the triplet staging area
-    sm.stA[lane] = d;
-    sm.stA[32 + lane] = 0.25f * fc;
-    ((int*)sm.stB)[lane] = sj;
-    unsigned m = __ballot_sync(0xffffffffu, is_ang);
-    if (is_ang) {
-      int pos = na + warp_exclusive_prefix(m, lane);
-      if (pos < kCapA) {
-        float inv = 1.0f / fmaxf(d, 1e-5f);
-        sm.au[4 * pos + 0] = vx * inv;
-        sm.au[4 * pos + 1] = vy * inv;
-        sm.au[4 * pos + 2] = vz * inv;
-        sm.au[4 * pos + 3] = d;
-        sm.afc[pos] = d < K.rca ? 0.5f * cosf(d * K.pi_rca) + 0.5f : 0.f;
-        sm.asp[pos] = sj;
-      }
-    }
-    na += __popc(m);
-    __syncwarp();
-    int nt = min(32, cnt - k0);
-    for (int t = h_lane; t < nt; t += nh) {
-      int s = ((int*)sm.stB)[t];
-      float dd = sm.stA[t] - sr;
-      float v = sm.stA[32 + t] * expf(-eta_r * dd * dd);
-      sm.rad[s * 32 + lane] += v;
-    }
-    __syncwarp();
-  }
+  int cnt_r, off_r, cnt_a, off_a, na;
+  stage_row<false>(st, st.cntw, xyzs, pi, c, nbr_j, nbr_shift, (size_t)i * cap, cnt, K, lane, cnt_r, off_r, cnt_a,
+                   off_a, na);
   if (lane == 0) {
     status_max(status, ST_ANG_MAXCOUNT, na);
     if (na > kCapA) status_set(status, ST_ANG_OVERFLOW);
   }
-  if (na > kCapA) na = kCapA;
+  const size_t orow = (size_t)atom_row[i] * ld;
 
-  // ---- angular terms over all unordered neighbour pairs -----------------------
-  const int T = na * (na - 1) / 2;
-  const int fr = lane / AS, fz = lane % AS;  // feature (r, z) of this lane
-  for (int t0 = 0; t0 < T; t0 += 32) {
-    int t = t0 + lane;
-    int p = -1;
-    if (t < T) {
-      int a, b;
-      triplet_ab(t, a, b);
-      float ax = sm.au[4 * a], ay = sm.au[4 * a + 1], az = sm.au[4 * a + 2], da = sm.au[4 * a + 3];
-      float bx = sm.au[4 * b], by = sm.au[4 * b + 1], bz = sm.au[4 * b + 2], db = sm.au[4 * b + 3];
-      float cosang = ax * bx + ay * by + az * bz;
-      float ct = 0.95f * cosang;
-      float st = sqrtf(fmaxf(1.0f - ct * ct, 0.f));
-      float f = K.c_ang * sm.afc[a] * sm.afc[b];
-#pragma unroll
-      for (int z = 0; z < AS; ++z) {
-        float cz = ct * K.cosz[z] + st * K.sinz[z];
-        sm.stA[lane * 33 + z] = f * powf(fmaxf(1.0f + cz, 0.f), K.zeta);
-      }
-      float dm = 0.5f * (da + db);
-#pragma unroll
-      for (int r = 0; r < AD; ++r) {
-        float x = dm - K.shift_a[r];
-        sm.stB[lane * 33 + r] = expf(-K.eta_a * x * x);
-      }
-      p = triu_pair(sm.asp[a], sm.asp[b], S);
+  // ---- radial: lane (r, h) accumulates feature r over the neighbours h, h+nh, ...
+  constexpr int nh = 32 / RD;
+  const int r_lane = lane % RD, h_lane = lane / RD;
+  const float sr = K.shift_r[r_lane], eta_r = K.eta_r;
+  for (int s = 0; s < S; ++s) {
+    const int ns = __shfl_sync(0xffffffffu, cnt_r, s);
+    const int os = __shfl_sync(0xffffffffu, off_r, s);
+    float acc = 0.f;
+    for (int t = h_lane; t < ns; t += nh) {
+      float2 e = st.rd[os + t];
+      float x = e.x - sr;
+      acc = fmaf(e.y, fexp(-eta_r * x * x), acc);
     }
-    sm.stP[lane] = p;
-    __syncwarp();
-    int nt = min(32, T - t0);
-    float* acc_col = sm.ang + lane;
-    for (int tt = 0; tt < nt; ++tt) {
-      int pp = sm.stP[tt];
-      acc_col[pp * 32] += sm.stA[tt * 33 + fz] * sm.stB[tt * 33 + fr];
-    }
-    __syncwarp();
+    if (nh == 2) acc += __shfl_xor_sync(0xffffffffu, acc, 16);
+    if (h_lane == 0) store_feature(out_kind, out, out_lo, orow + s * RD + r_lane, acc);
   }
 
-  // ---- write the AEV row ------------------------------------------------------
-  const size_t orow = (size_t)atom_row[i] * ld;
-  const int F = K.F, FR = S * RD;
-  for (int col = lane; col < F; col += 32) {
-    float v;
-    if (col < FR) {
-      int s = col / RD, r = col % RD;
-      v = 0.f;
-      for (int h = 0; h < nh; ++h) v += sm.rad[s * 32 + r + RD * h];
-    } else {
-      v = sm.ang[col - FR];
-    }
-    if (out_kind == FENNOL_AEV_F32) {
-      ((float*)out)[orow + col] = v;
-    } else {
-      __nv_bfloat16 hi = to_bf16(v);
-      ((__nv_bfloat16*)out)[orow + col] = hi;
-      if (out_kind == FENNOL_AEV_BF16X2)
-        ((__nv_bfloat16*)out_lo)[orow + col] = to_bf16(v - __bfloat162float(hi));
+  // ---- angular: zero every species-pair block, then fill the present ones
+  const int FR = S * RD;
+  for (int col = lane; col < K.P * 32; col += 32) store_feature(out_kind, out, out_lo, orow + FR + col, 0.f);
+  const float c_ang = K.c_ang, eta_a = K.eta_a;
+  const unsigned present = __ballot_sync(0xffffffffu, lane < S && cnt_a > 0);
+  for (unsigned m1 = present; m1; m1 &= m1 - 1) {
+    const int s1 = __ffs(m1) - 1;
+    const int n1 = min(__shfl_sync(0xffffffffu, cnt_a, s1), kCapA);
+    const int o1 = __shfl_sync(0xffffffffu, off_a, s1);
+    for (unsigned m2 = m1; m2; m2 &= m2 - 1) {
+      const int s2 = __ffs(m2) - 1;
+      const int n2 = min(__shfl_sync(0xffffffffu, cnt_a, s2), kCapA);
+      const int o2 = __shfl_sync(0xffffffffu, off_a, s2);
+      int T = s1 == s2 ? n1 * (n1 - 1) / 2 : n1 * n2;
+      if (o1 + n1 > kCapA || o2 + n2 > kCapA) T = 0;  // overflowing atom: reported above
+      if (T == 0) continue;
+      const int p = triu_pair(s1, s2, S);
+      float acc[32];
+#pragma unroll
+      for (int k = 0; k < 32; ++k) acc[k] = 0.f;
+      for (int t0 = 0; t0 < T; t0 += 32) {
+        const int t = t0 + lane;
+        if (t < T) {
+          int a, b;
+          if (s1 == s2) {
+            tri_ab(t, a, b);
+            a += o1;
+            b += o1;
+          } else {
+            a = o1 + t / n2;
+            b = o2 + t % n2;
+          }
+          const float4 ua = st.au[a], ub = st.au[b];
+          const float cosang = ua.x * ub.x + ua.y * ub.y + ua.z * ub.z;
+          const float ct = 0.95f * cosang;
+          const float stt = sqrtf(fmaxf(1.0f - ct * ct, 0.f));
+          const float f = c_ang * st.af[a].x * st.af[b].x;
+          float A[AS], B[AD];
+#pragma unroll
+          for (int z = 0; z < AS; ++z) {
+            float cz = ct * K.cosz[z] + stt * K.sinz[z];
+            A[z] = f * zeta_pow(1.0f + cz, K.zeta_n, K.zeta_f);
+          }
+          const float dm = 0.5f * (ua.w + ub.w);
+#pragma unroll
+          for (int r = 0; r < AD; ++r) {
+            float x = dm - K.shift_a[r];
+            B[r] = fexp(-eta_a * x * x);
+          }
+#pragma unroll
+          for (int r = 0; r < AD; ++r)
+#pragma unroll
+            for (int z = 0; z < AS; ++z) acc[r * AS + z] = fmaf(A[z], B[r], acc[r * AS + z]);
+        }
+      }
+      const float v = transpose_reduce32(acc, lane);
+      __syncwarp();
+      store_feature(out_kind, out, out_lo, orow + FR + p * 32 + lane, v);
     }
   }
 }
@@ -275,180 +421,153 @@ k_aev_forward(const float4* __restrict__ xyzs, int n, const int* __restrict__ at
 // --------------------------------------------------------------------------------
 // Adjoint: dE/dAEV -> forces.
 // --------------------------------------------------------------------------------
-__host__ __device__ __forceinline__ int bwd_smem_floats(int S, int P, int cap) {
-  return S * 33 + P * 33 + kCapA * 8 + cap * 4;
+__host__ __device__ __forceinline__ size_t bwd_bytes(int S, int RD, int cap) {
+  return (stage_bytes(cap) + (size_t)cap * 12 + (size_t)S * (RD + 1) * 4 + 15) / 16 * 16;
 }
 
 template <int RD, int AD, int AS>
-__global__ void __launch_bounds__(kAevWarps * 32)
+__global__ void __launch_bounds__(kAevWarps * 32, 3)
 k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ atom_sys,
                const float* __restrict__ sys_cell, const int* __restrict__ nbr_j,
                const unsigned* __restrict__ nbr_shift, const int* __restrict__ nbr_count, int cap,
                const AevConst K, const int* __restrict__ atom_row, const float* __restrict__ daev,
                int ld, float4* __restrict__ forces, int* status) {
-  extern __shared__ float smem[];
+  extern __shared__ __align__(16) char smem_c[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int i = blockIdx.x * kAevWarps + warp;
   if (i >= n) return;
-  const int S = K.S, P = K.P;
-  float* gr = smem + (size_t)warp * bwd_smem_floats(S, P, cap);  // [S][33]
-  float* ga = gr + S * 33;                                         // [P][33]
-  float* au = ga + P * 33;                                         // [kCapA][4]
-  float* afc = au + kCapA * 4;                                     // [kCapA]
-  float* adfc = afc + kCapA;                                       // [kCapA]
-  int* asp = (int*)(adfc + kCapA);                                 // [kCapA]
-  int* aslot = asp + kCapA;                                        // [kCapA]
-  float* grad = (float*)(aslot + kCapA);                           // [cap][4]
+  const int S = K.S;
+  char* base = smem_c + (size_t)warp * bwd_bytes(S, RD, cap);
+  Stage st = carve_stage(base, cap);
+  float* gxs = (float*)(base + stage_bytes(cap));                     // [cap] x, y, z gradients
+  float* gys = gxs + cap;
+  float* gzs = gys + cap;
+  float* gr = gzs + cap;                                              // [S][RD+1]
 
-  // dE/dAEV row -> shared memory (padded rows avoid bank conflicts)
   const float* g = daev + (size_t)atom_row[i] * ld;
   const int FR = S * RD;
-  for (int col = lane; col < FR; col += 32) gr[(col / RD) * 33 + col % RD] = g[col];
-  for (int col = lane; col < P * 32; col += 32) ga[(col >> 5) * 33 + (col & 31)] = g[FR + col];
-
+  for (int col = lane; col < FR; col += 32) gr[(col / RD) * (RD + 1) + col % RD] = g[col];
   const float4 pi = xyzs[i];
   float c[9];
   load_cell(sys_cell, atom_sys[i], c);
   int cnt = nbr_count[i];
   if (cnt > cap) cnt = cap;
   const size_t row = (size_t)i * cap;
-  __syncwarp();
+  int cnt_r, off_r, cnt_a, off_a, na;
+  stage_row<true>(st, st.cntw, xyzs, pi, c, nbr_j, nbr_shift, row, cnt, K, lane, cnt_r, off_r, cnt_a, off_a, na);
+  if (na > kCapA && lane == 0) status_set(status, ST_ANG_OVERFLOW);
 
-  // ---- radial: lane per neighbour --------------------------------------------
-  int na = 0;
-  for (int k0 = 0; k0 < cnt; k0 += 32) {
-    int k = k0 + lane;
-    bool is_ang = false;
-    float vx = 0.f, vy = 0.f, vz = 0.f, d = 1.f, d2 = 0.f;
-    int sj = 0;
-    if (k < cnt) {
-      int j = __ldg(nbr_j + row + k);
-      unsigned sh = __ldg(nbr_shift + row + k);
-      float4 pj = xyzs[j];
-      edge_vec(pi, pj, sh, c, vx, vy, vz);
-      d2 = dist2_exact(vx, vy, vz);
-      d = sqrtf(fmaxf(d2, 1e-5f));
-      sj = __float_as_int(pj.w);
-      float fc = 0.f, dfc = 0.f;
-      if (d < K.rc) {
-        float sa, ca;
-        sincosf(d * K.pi_rc, &sa, &ca);
-        fc = 0.5f * ca + 0.5f;
-        dfc = -0.5f * K.pi_rc * sa;
-      }
-      float dEdd = 0.f;
-      const float* grow = gr + sj * 33;
+  // ---- radial: lane per neighbour (row order), gradient into grad[k]
+  for (int k = lane; k < cnt; k += 32) {
+    const float4 v = st.tmp[k];
+    const int sj = st.tkey[k] & 0xFF;
+    const float d = sqrtf(fmaxf(v.w, 1e-5f));
+    float fc = 0.f, dfc = 0.f;
+    if (d < K.rc) {
+      float sa, ca;
+      sincosf(d * K.pi_rc, &sa, &ca);
+      fc = 0.5f * ca + 0.5f;
+      dfc = -0.5f * K.pi_rc * sa;
+    }
+    const float* grow = gr + sj * (RD + 1);
+    float dEdd = 0.f;
 #pragma unroll 8
-      for (int r = 0; r < RD; ++r) {
-        float x = d - K.shift_r[r];
-        float e = expf(-K.eta_r * x * x);
-        dEdd += grow[r] * e * (dfc - 2.f * K.eta_r * x * fc);
-      }
-      dEdd *= 0.25f;
-      float s = d2 > 1e-5f ? dEdd / d : 0.f;
-      grad[4 * k + 0] = s * vx;
-      grad[4 * k + 1] = s * vy;
-      grad[4 * k + 2] = s * vz;
-      is_ang = d2 < K.rca2;
+    for (int r = 0; r < RD; ++r) {
+      float x = d - K.shift_r[r];
+      float e = fexp(-K.eta_r * x * x);
+      dEdd = fmaf(grow[r] * e, dfc - 2.f * K.eta_r * x * fc, dEdd);
     }
-    unsigned m = __ballot_sync(0xffffffffu, is_ang);
-    if (is_ang) {
-      int pos = na + warp_exclusive_prefix(m, lane);
-      if (pos < kCapA) {
-        float inv = 1.0f / fmaxf(d, 1e-5f);
-        au[4 * pos + 0] = vx * inv;
-        au[4 * pos + 1] = vy * inv;
-        au[4 * pos + 2] = vz * inv;
-        au[4 * pos + 3] = d;
-        float fc = 0.f, dfc = 0.f;
-        if (d < K.rca) {
-          float sa, ca;
-          sincosf(d * K.pi_rca, &sa, &ca);
-          fc = 0.5f * ca + 0.5f;
-          dfc = -0.5f * K.pi_rca * sa;
+    float sc = v.w > 1e-5f ? 0.25f * dEdd / d : 0.f;
+    gxs[k] = sc * v.x;
+    gys[k] = sc * v.y;
+    gzs[k] = sc * v.z;
+  }
+  __syncwarp();
+
+  // ---- angular: present species-pair blocks, lane per triplet
+  const float zeta = K.zeta, c_ang = K.c_ang, eta_a = K.eta_a;
+  const unsigned present = __ballot_sync(0xffffffffu, lane < S && cnt_a > 0);
+  for (unsigned m1 = present; m1; m1 &= m1 - 1) {
+    const int s1 = __ffs(m1) - 1;
+    const int n1 = min(__shfl_sync(0xffffffffu, cnt_a, s1), kCapA);
+    const int o1 = __shfl_sync(0xffffffffu, off_a, s1);
+    for (unsigned m2 = m1; m2; m2 &= m2 - 1) {
+      const int s2 = __ffs(m2) - 1;
+      const int n2 = min(__shfl_sync(0xffffffffu, cnt_a, s2), kCapA);
+      const int o2 = __shfl_sync(0xffffffffu, off_a, s2);
+      int T = s1 == s2 ? n1 * (n1 - 1) / 2 : n1 * n2;
+      if (o1 + n1 > kCapA || o2 + n2 > kCapA) T = 0;
+      if (T == 0) continue;
+      const int p = triu_pair(s1, s2, S);
+      float G[32];
+      const float* gp = g + FR + p * 32;
+#pragma unroll
+      for (int k = 0; k < 32; ++k) G[k] = __ldg(gp + k);
+      for (int t = lane; t < T; t += 32) {
+        int a, b;
+        if (s1 == s2) {
+          diag_ab(t, n1, a, b);
+          a += o1;
+          b += o1;
+        } else {
+          const int aa = t % n1, dd = t / n1;
+          a = o1 + aa;
+          b = o2 + (aa + dd) % n2;
         }
-        afc[pos] = fc;
-        adfc[pos] = dfc;
-        asp[pos] = sj;
-        aslot[pos] = k;
+        const float4 ua = st.au[a], ub = st.au[b];
+        const float2 fa2 = st.af[a], fb2 = st.af[b];
+        const float cosang = ua.x * ub.x + ua.y * ub.y + ua.z * ub.z;
+        const float ct = 0.95f * cosang;
+        const float stt = sqrtf(fmaxf(1.0f - ct * ct, 1e-12f));
+        float A[AS], Ap[AS];
+#pragma unroll
+        for (int z = 0; z < AS; ++z) {
+          float cz = ct * K.cosz[z] + stt * K.sinz[z];
+          float sz = stt * K.cosz[z] - ct * K.sinz[z];
+          float bs = fmaxf(1.0f + cz, 0.f);
+          float pw1 = zeta_pow(bs, K.zeta1_n, K.zeta1_f);
+          A[z] = pw1 * bs;
+          Ap[z] = -zeta * pw1 * sz;
+        }
+        const float dm = 0.5f * (ua.w + ub.w);
+        float Q = 0.f, Th = 0.f, Dm = 0.f;
+#pragma unroll
+        for (int r = 0; r < AD; ++r) {
+          float x = dm - K.shift_a[r];
+          float Bv = fexp(-eta_a * x * x);
+          float GA = 0.f, GAp = 0.f;
+#pragma unroll
+          for (int z = 0; z < AS; ++z) {
+            GA = fmaf(G[r * AS + z], A[z], GA);
+            GAp = fmaf(G[r * AS + z], Ap[z], GAp);
+          }
+          Q = fmaf(GA, Bv, Q);
+          Th = fmaf(GAp, Bv, Th);
+          Dm = fmaf(GA, -2.f * eta_a * x * Bv, Dm);
+        }
+        const float fa = fa2.x, fb = fb2.x;
+        const float cfab = c_ang * fa * fb;
+        const float dEddm = cfab * Dm;
+        const float dEdda = 0.5f * dEddm + c_ang * fb * Q * fa2.y;
+        const float dEddb = 0.5f * dEddm + c_ang * fa * Q * fb2.y;
+        const float dEdc = cfab * Th * (-0.95f / stt);
+        const float ia = dEdc / ua.w, ib = dEdc / ub.w;
+        const int sa_ = st.aslot[a], sb_ = st.aslot[b];
+        atomicAdd(gxs + sa_, dEdda * ua.x + ia * (ub.x - cosang * ua.x));
+        atomicAdd(gys + sa_, dEdda * ua.y + ia * (ub.y - cosang * ua.y));
+        atomicAdd(gzs + sa_, dEdda * ua.z + ia * (ub.z - cosang * ua.z));
+        atomicAdd(gxs + sb_, dEddb * ub.x + ib * (ua.x - cosang * ub.x));
+        atomicAdd(gys + sb_, dEddb * ub.y + ib * (ua.y - cosang * ub.y));
+        atomicAdd(gzs + sb_, dEddb * ub.z + ib * (ua.z - cosang * ub.z));
       }
     }
-    na += __popc(m);
-  }
-  if (na > kCapA) {
-    if (lane == 0) status_set(status, ST_ANG_OVERFLOW);
-    na = kCapA;
   }
   __syncwarp();
 
-  // ---- angular: lane per triplet -----------------------------------------------
-  const int T = na * (na - 1) / 2;
-  const float zeta = K.zeta;
-  for (int t = lane; t < T; t += 32) {
-    int a, b;
-    triplet_ab(t, a, b);
-    float uax = au[4 * a], uay = au[4 * a + 1], uaz = au[4 * a + 2], da = au[4 * a + 3];
-    float ubx = au[4 * b], uby = au[4 * b + 1], ubz = au[4 * b + 2], db = au[4 * b + 3];
-    float cosang = uax * ubx + uay * uby + uaz * ubz;
-    float ct = 0.95f * cosang;
-    float st = sqrtf(fmaxf(1.0f - ct * ct, 1e-12f));
-    int p = triu_pair(asp[a], asp[b], S);
-    const float* gp = ga + p * 33;
-    float A[AS], Ap[AS];
-#pragma unroll
-    for (int z = 0; z < AS; ++z) {
-      float cz = ct * K.cosz[z] + st * K.sinz[z];
-      float sz = st * K.cosz[z] - ct * K.sinz[z];  // sin(theta - Z)
-      float base = fmaxf(1.0f + cz, 0.f);
-      float pw1 = base > 0.f ? powf(base, zeta - 1.0f) : 0.f;
-      A[z] = pw1 * base;
-      Ap[z] = -zeta * pw1 * sz;
-    }
-    float dm = 0.5f * (da + db);
-    float Q = 0.f, Th = 0.f, Dm = 0.f;
-#pragma unroll
-    for (int r = 0; r < AD; ++r) {
-      float x = dm - K.shift_a[r];
-      float B = expf(-K.eta_a * x * x);
-      float GA = 0.f, GAp = 0.f;
-#pragma unroll
-      for (int z = 0; z < AS; ++z) {
-        float gv = gp[r * AS + z];
-        GA += gv * A[z];
-        GAp += gv * Ap[z];
-      }
-      Q += GA * B;
-      Th += GAp * B;
-      Dm += GA * (-2.f * K.eta_a * x * B);
-    }
-    float fa = afc[a], fb = afc[b];
-    float C = K.c_ang;
-    float dEdth = C * fa * fb * Th;
-    float dEddm = C * fa * fb * Dm;
-    float dEdda = 0.5f * dEddm + C * fb * Q * adfc[a];
-    float dEddb = 0.5f * dEddm + C * fa * Q * adfc[b];
-    float dEdc = dEdth * (-0.95f / st);
-    float ia = dEdc / da, ib = dEdc / db;
-    float gax = dEdda * uax + ia * (ubx - cosang * uax);
-    float gay = dEdda * uay + ia * (uby - cosang * uay);
-    float gaz = dEdda * uaz + ia * (ubz - cosang * uaz);
-    float gbx = dEddb * ubx + ib * (uax - cosang * ubx);
-    float gby = dEddb * uby + ib * (uay - cosang * uby);
-    float gbz = dEddb * ubz + ib * (uaz - cosang * ubz);
-    int sa_ = aslot[a], sb_ = aslot[b];
-    atomicAdd(grad + 4 * sa_ + 0, gax);
-    atomicAdd(grad + 4 * sa_ + 1, gay);
-    atomicAdd(grad + 4 * sa_ + 2, gaz);
-    atomicAdd(grad + 4 * sb_ + 0, gbx);
-    atomicAdd(grad + 4 * sb_ + 1, gby);
-    atomicAdd(grad + 4 * sb_ + 2, gbz);
-  }
-  __syncwarp();
-
-  // ---- scatter: F_j -= g, F_i += sum g ----------------------------------------
+  // ---- scatter: F_j -= g, F_i += sum g
   float fx = 0.f, fy = 0.f, fz = 0.f;
   for (int k = lane; k < cnt; k += 32) {
-    float gx = grad[4 * k], gy = grad[4 * k + 1], gz = grad[4 * k + 2];
+    const float gx = gxs[k], gy = gys[k], gz = gzs[k];
     int j = __ldg(nbr_j + row + k);
     atomicAdd(forces + j, make_float4(-gx, -gy, -gz, 0.f));
     fx += gx;
@@ -487,10 +606,20 @@ bool dispatch(const AevConst& K, Fn&& fn) {
   return false;
 }
 
+// Opt a kernel in to the largest dynamic shared memory it can use, once.
 size_t set_smem(const void* fn, size_t bytes) {
+  static const void* done[16] = {};
   if (bytes > 48 * 1024) {
-    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess)
-      return 0;
+    for (int k = 0; k < 16; ++k) {
+      if (done[k] == fn) return bytes;
+      if (!done[k]) {
+        if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess)
+          return 0;
+        done[k] = fn;
+        return bytes;
+      }
+    }
+    return 0;
   }
   return bytes;
 }
@@ -527,10 +656,10 @@ extern "C" int fennol_aev_forward(const float* xyzs, int natoms, const int* atom
   if (out_kind != FENNOL_AEV_F32 && out_kind != FENNOL_AEV_BF16 && out_kind != FENNOL_AEV_BF16X2)
     return FENNOL_ERR_INVALID;
   if (out_kind == FENNOL_AEV_BF16X2 && !out_lo) return FENNOL_ERR_INVALID;
+  if ((size_t)kAevWarps * stage_bytes(capacity) > 200 * 1024) return FENNOL_ERR_UNSUPPORTED;
   int blocks = (natoms + kAevWarps - 1) / kAevWarps;
   bool launched = dispatch(K, [&](auto ks) {
-    size_t smem = set_smem((const void*)ks.fwd,
-                           (size_t)kAevWarps * fwd_smem_floats(K.S, K.P) * sizeof(float));
+    size_t smem = set_smem((const void*)ks.fwd, (size_t)kAevWarps * stage_bytes(capacity));
     if (!smem) return false;
     ks.fwd<<<blocks, kAevWarps * 32, smem, (cudaStream_t)stream>>>(
         (const float4*)xyzs, natoms, atom_sys, sys_cell, nbr_j, nbr_shift, nbr_count, capacity, K,
@@ -553,7 +682,7 @@ extern "C" int fennol_aev_backward(const float* xyzs, int natoms, const int* ato
   if (natoms == 0) return FENNOL_OK;
   if (!xyzs || !atom_sys || !nbr_j || !nbr_shift || !nbr_count || !atom_row || !daev || !forces4)
     return FENNOL_ERR_INVALID;
-  size_t bytes = (size_t)kAevWarps * bwd_smem_floats(K.S, K.P, capacity) * sizeof(float);
+  size_t bytes = (size_t)kAevWarps * bwd_bytes(K.S, K.RD, capacity);
   if (bytes > 200 * 1024) return FENNOL_ERR_UNSUPPORTED;
   int blocks = (natoms + kAevWarps - 1) / kAevWarps;
   bool launched = dispatch(K, [&](auto ks) {
