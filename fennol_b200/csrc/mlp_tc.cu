@@ -8,8 +8,13 @@
 //               swizzle) into a multi-stage shared-memory ring;
 //   warp 1      allocates the TMEM accumulator, one thread issues
 //               tcgen05.mma (M=128, N=bn, K=16) and tcgen05.commit;
-//   warps 2-5   epilogue: tcgen05.ld of the FP32 accumulator (one row per
-//               thread), fused bias + CELU / CELU' / energy head, and stores.
+//   warps 2-9   epilogue: tcgen05.ld of the FP32 accumulator (one row per
+//               thread, two warps per TMEM lane quarter splitting the
+//               columns), fused bias + CELU / CELU' / energy head, stores.
+// Launches use programmatic dependent launch: a kernel's prologue (barrier
+// init, TMEM allocation) and its first weight tiles overlap the tail of the
+// previous kernel; inputs written by that kernel are read only after
+// griddepcontrol.wait.
 // Split-BF16 operands: activations are carried as hi + lo bfloat16 pairs
 // (x = hi + lo to ~16 bits) and, in the 3-product form, weights too:
 // acc += A_hi B_hi + A_lo B_hi (+ A_hi B_lo), all accumulated in FP32 TMEM.
@@ -30,7 +35,8 @@ using namespace fnl::umma;
 
 namespace {
 
-constexpr int kThreads = 192;
+constexpr int kThreads = 320;
+constexpr int kEpiThreads = 256;
 constexpr int BM = 128, BK = 64;
 constexpr uint64_t kTimeoutNs = 2000000000ull;
 constexpr int kSmemBudget = 220 * 1024;
@@ -60,13 +66,21 @@ struct TcParams {
   int ld_out;
   const __nv_bfloat16* act_hi;  // EPI_DACT: forward activation of this layer
   const __nv_bfloat16* act_lo;
-  float* e_rows;
+  float* e_part;        // EPI_HEAD: [slot][rows] partial energies (slot = model*n_chunks + chunk)
+  int slot_base;
+  int rows;
   float* out_f32;
   int ld_f32;
   int* err;
 };
 
 __device__ __forceinline__ float dcelu_from_z(float z, float alpha) { return z > 0.f ? 1.f : __expf(z / alpha); }
+__device__ __forceinline__ float celu_fast(float x, float alpha) {
+  return x > 0.f ? x : alpha * (__expf(x / alpha) - 1.f);
+}
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, %0;" ::"n"(kEpiThreads) : "memory"); }
 
 __device__ __forceinline__ void split_store(__nv_bfloat16* hi, __nv_bfloat16* lo, const float* v) {
   // 32 values -> 64 bytes of hi (and lo) as four 16-byte stores each
@@ -145,6 +159,7 @@ k_umma_gemm(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
   fence_after_sync();
   const uint32_t tmem = *tmem_slot;
   bool failed = false;
+  griddep_launch();
 
   auto stage_a = [&](int s) { return smem + (size_t)s * stage_bytes; };
   auto stage_alo = [&](int s) { return smem + (size_t)s * stage_bytes + a_bytes; };
@@ -153,9 +168,21 @@ k_umma_gemm(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
 
   if (warp == 0) {
     if (lane == 0) {
-      for (int kc = 0; kc < p.nk; ++kc) {
+      // weights do not depend on the previous kernel: fetch the first stages now
+      const int pre = p.nk < p.stages ? p.nk : p.stages;
+      for (int kc = 0; kc < pre; ++kc) {
+        mbar_expect_tx(full + kc, stage_bytes);
+        tma_load_2d(&mapB, full + kc, stage_b(kc), kc * BK, b_row);
+        if (p.b_lo) tma_load_2d(&mapBlo, full + kc, stage_blo(kc), kc * BK, b_row);
+      }
+      griddep_wait();
+      for (int kc = 0; kc < pre; ++kc) {
+        tma_load_2d(&mapA, full + kc, stage_a(kc), kc * BK, a_row);
+        if (p.a_lo) tma_load_2d(&mapAlo, full + kc, stage_alo(kc), kc * BK, a_row);
+      }
+      for (int kc = pre; kc < p.nk; ++kc) {
         int s = kc % p.stages, u = kc / p.stages;
-        if (u > 0 && !mbar_wait(empty + s, (u - 1) & 1, deadline)) {
+        if (!mbar_wait(empty + s, (u - 1) & 1, deadline)) {
           failed = true;
           break;
         }
@@ -190,26 +217,28 @@ k_umma_gemm(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
       mma_commit(accum);
     }
   } else {
-    // epilogue: 4 warps, TMEM lane quarter = warp % 4
+    // epilogue: 8 warps; TMEM lane quarter = warp % 4, column half = (warp - 2) / 4
     const int q = warp & 3;
+    const int half = (warp - 2) >> 2;
     const int r = 32 * q + lane;
     const int row = a_row + r;
+    griddep_wait();
     // warp-uniform decision: tcgen05.ld below is a warp-collective instruction
     const bool ready = __all_sync(0xffffffffu, mbar_wait(accum, 0, deadline));
+    float e = 0.f;
     if (!ready) {
       failed = true;
     } else {
       fence_after_sync();
-      float e = 0.f;
       const float* bias = p.bias ? p.bias + (size_t)grp * p.n_full : nullptr;
       const float* w4 = p.w4 ? p.w4 + (size_t)grp * p.n_full : nullptr;
-      for (int cc = 0; cc < p.bn / 32; ++cc) {
+      for (int cc = half; cc < p.bn / 32; cc += 2) {
         float v[32];
         tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(cc * 32), v);
         const int n = n0 + cc * 32;
         if (EPI == EPI_HIDDEN) {
 #pragma unroll
-          for (int k = 0; k < 32; ++k) v[k] = celu_f(v[k] + __ldg(bias + n + k), p.alpha);
+          for (int k = 0; k < 32; ++k) v[k] = celu_fast(v[k] + __ldg(bias + n + k), p.alpha);
           split_store(p.out_hi + (size_t)row * p.ld_out + n,
                       p.out_lo ? p.out_lo + (size_t)row * p.ld_out + n : nullptr, v);
         } else if (EPI == EPI_HEAD) {
@@ -217,7 +246,7 @@ k_umma_gemm(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
           for (int k = 0; k < 32; ++k) {
             float z = v[k] + __ldg(bias + n + k);
             float wv = __ldg(w4 + n + k);
-            e = fmaf(celu_f(z, p.alpha), wv, e);
+            e = fmaf(celu_fast(z, p.alpha), wv, e);
             v[k] = wv * dcelu_from_z(z, p.alpha);
           }
           split_store(p.out_hi + (size_t)row * p.ld_out + n,
@@ -251,9 +280,16 @@ k_umma_gemm(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CU
           }
         }
       }
-      if (EPI == EPI_HEAD) {
-        float prev = p.first_model ? 0.f : p.e_rows[row];
-        p.e_rows[row] = prev + (e + __ldg(p.b4 + grp)) * p.inv_models;
+    }
+    if (EPI == EPI_HEAD) {
+      // combine the two column halves of this row, then one partial per (model, chunk)
+      float* ex = reinterpret_cast<float*>(tmem_slot + 4);
+      if (half == 1) ex[r] = e;
+      epi_bar();
+      if (half == 0 && ready) {
+        e += ex[r];
+        if (chunk == 0) e += __ldg(p.b4 + grp);
+        p.e_part[(size_t)(p.slot_base + chunk) * p.rows + row] = e;
       }
     }
   }
@@ -342,7 +378,7 @@ int launch_epi(const Gemm& g, int rows, int ntiles, cudaStream_t st) {
   uint32_t cols = 32;
   while (cols < (uint32_t)g.bn) cols <<= 1;
   p.tmem_cols = cols;
-  size_t smem = (size_t)stages * stage + 1024 + 256;
+  size_t smem = (size_t)stages * stage + 1024 + 1024;
   static bool attr_set = false;
   if (!attr_set) {
     if (cudaFuncSetAttribute(k_umma_gemm<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBudget + 2048) !=
@@ -350,8 +386,17 @@ int launch_epi(const Gemm& g, int rows, int ntiles, cudaStream_t st) {
       return FENNOL_ERR_CUDA;
     attr_set = true;
   }
-  k_umma_gemm<EPI><<<ntiles * p.n_chunks, kThreads, smem, st>>>(ma, mal, mb, mbl, p);
-  FNL_CHECK_LAUNCH();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(ntiles * p.n_chunks);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (cudaLaunchKernelEx(&cfg, k_umma_gemm<EPI>, ma, mal, mb, mbl, p) != cudaSuccess) return FENNOL_ERR_CUDA;
   return FENNOL_OK;
 }
 
@@ -367,9 +412,23 @@ int launch(const Gemm& g, int rows, int ntiles, cudaStream_t st) {
 struct TcWs {
   int* err;
   __nv_bfloat16 *h1, *h1l, *h2, *h2l, *g3, *g3l;
+  float* e_part;  // [n_models * kHeadChunks][rows]
 };
 
+constexpr int kHeadChunks = 2;
+
+// e_rows[r] = sum over (model, chunk) partials / n_models, fixed order.
+__global__ void k_e_rows(const float* __restrict__ e_part, int slots, int rows, float inv_models,
+                         float* __restrict__ e_rows) {
+  int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  float e = 0.f;
+  for (int k = 0; k < slots; ++k) e += e_part[(size_t)k * rows + r];
+  e_rows[r] = e * inv_models;
+}
+
 size_t tc_layout(int rows, const fennol_mlp_weights* w, char* base, TcWs* out) {
+  const size_t ep = (size_t)w->n_models * kHeadChunks * rows * sizeof(float);
   size_t off = 256;
   auto take = [&](size_t bytes) {
     size_t o = off;
@@ -379,6 +438,7 @@ size_t tc_layout(int rows, const fennol_mlp_weights* w, char* base, TcWs* out) {
   size_t d1 = (size_t)rows * w->dims[1] * 2, d2 = (size_t)rows * w->dims[2] * 2,
          d3 = (size_t)rows * w->dims[3] * 2;
   size_t o1 = take(d1), o1l = take(d1), o2 = take(d2), o2l = take(d2), o3 = take(d3), o3l = take(d3);
+  size_t oe = take(ep);
   if (base && out) {
     out->err = (int*)base;
     out->h1 = (__nv_bfloat16*)(base + o1);
@@ -387,6 +447,7 @@ size_t tc_layout(int rows, const fennol_mlp_weights* w, char* base, TcWs* out) {
     out->h2l = (__nv_bfloat16*)(base + o2l);
     out->g3 = (__nv_bfloat16*)(base + o3);
     out->g3l = (__nv_bfloat16*)(base + o3l);
+    out->e_part = (float*)(base + oe);
   }
   return off;
 }
@@ -449,32 +510,34 @@ int fnl_mlp_tc(int precision, int rows, int ntiles, const int* tile_species, con
     const int g0 = m * w->n_species;
     int rc;
     // L1: H1 = celu(X W1 + b1)
-    Gemm g = base(EPI_HIDDEN, x, x_lo, d[0], w->wt_hi[0], w->wt_lo[0], d[1], d[1], d[1], g0);
+    Gemm g = base(EPI_HIDDEN, x, x_lo, d[0], w->wt_hi[0], w->wt_lo[0], d[1], d[1], d[1] / 2, g0);
     g.p.bias = w->b32[0];
     g.p.out_hi = t.h1;
     g.p.out_lo = t.h1l;
     g.p.ld_out = d[1];
     if ((rc = launch(g, rows, ntiles, st))) return rc;
     // L2: H2 = celu(H1 W2 + b2)
-    g = base(EPI_HIDDEN, t.h1, t.h1l, d[1], w->wt_hi[1], w->wt_lo[1], d[2], d[2], d[2], g0);
+    g = base(EPI_HIDDEN, t.h1, t.h1l, d[1], w->wt_hi[1], w->wt_lo[1], d[2], d[2], d[2] / 2, g0);
     g.p.bias = w->b32[1];
     g.p.out_hi = t.h2;
     g.p.out_lo = t.h2l;
     g.p.ld_out = d[2];
     if ((rc = launch(g, rows, ntiles, st))) return rc;
     // L3 + head: e = celu(H2 W3 + b3) . w4 + b4 ; G3 = w4 * celu'(z3)
-    g = base(EPI_HEAD, t.h2, t.h2l, d[2], w->wt_hi[2], w->wt_lo[2], d[3], d[3], d[3], g0);
+    g = base(EPI_HEAD, t.h2, t.h2l, d[2], w->wt_hi[2], w->wt_lo[2], d[3], d[3], d[3] / kHeadChunks, g0);
     g.p.bias = w->b32[2];
     g.p.w4 = w->w32[3];
     g.p.b4 = w->b32[3];
     g.p.out_hi = t.g3;
     g.p.out_lo = t.g3l;
     g.p.ld_out = d[3];
-    g.p.e_rows = e_rows;
+    g.p.e_part = t.e_part;
+    g.p.slot_base = m * kHeadChunks;
+    g.p.rows = rows;
     g.p.first_model = m == 0;
     if ((rc = launch(g, rows, ntiles, st))) return rc;
     // B3: G2 = (G3 W3^T) * celu'(H2), in place of H2
-    g = base(EPI_DACT, t.g3, t.g3l, d[3], w->w_hi[2], w->w_lo[2], d[2], d[2], d[2], g0);
+    g = base(EPI_DACT, t.g3, t.g3l, d[3], w->w_hi[2], w->w_lo[2], d[2], d[2], d[2] / 2, g0);
     g.p.act_hi = t.h2;
     g.p.act_lo = t.h2l;
     g.p.out_hi = t.h2;
@@ -482,7 +545,7 @@ int fnl_mlp_tc(int precision, int rows, int ntiles, const int* tile_species, con
     g.p.ld_out = d[2];
     if ((rc = launch(g, rows, ntiles, st))) return rc;
     // B2: G1 = (G2 W2^T) * celu'(H1), in place of H1
-    g = base(EPI_DACT, t.h2, t.h2l, d[2], w->w_hi[1], w->w_lo[1], d[1], d[1], d[1], g0);
+    g = base(EPI_DACT, t.h2, t.h2l, d[2], w->w_hi[1], w->w_lo[1], d[1], d[1], d[1] / 2, g0);
     g.p.act_hi = t.h1;
     g.p.act_lo = t.h1l;
     g.p.out_hi = t.h1;
@@ -490,11 +553,13 @@ int fnl_mlp_tc(int precision, int rows, int ntiles, const int* tile_species, con
     g.p.ld_out = d[1];
     if ((rc = launch(g, rows, ntiles, st))) return rc;
     // B1: dX (+)= (G1 W1^T) / n_models
-    g = base(EPI_OUT, t.h1, t.h1l, d[1], w->w_hi[0], w->w_lo[0], d[0], d[0], 256, g0);
+    g = base(EPI_OUT, t.h1, t.h1l, d[1], w->w_hi[0], w->w_lo[0], d[0], d[0], 128, g0);
     g.p.out_f32 = dx;
     g.p.ld_f32 = d[0];
     g.p.first_model = m == 0;
     if ((rc = launch(g, rows, ntiles, st))) return rc;
   }
+  k_e_rows<<<(rows + 255) / 256, 256, 0, st>>>(t.e_part, w->n_models * kHeadChunks, rows, inv_m, e_rows);
+  FNL_CHECK_LAUNCH();
   return FENNOL_OK;
 }
