@@ -25,3 +25,8 @@ size_t fnl_mlp_tc_workspace(int precision, int rows, int n_models, const fennol_
 int fnl_mlp_tc(int precision, int rows, int ntiles, const int* tile_species, const int* tile_row,
                const fennol_mlp_weights* w, const void* x, const void* x_lo, float* e_rows, float* dx,
                void* ws, size_t ws_bytes, cudaStream_t st);
+bool fnl_mlp_fused_supported(int precision, const fennol_mlp_weights* w);
+size_t fnl_mlp_fused_workspace(const fennol_mlp_weights* w);
+int fnl_mlp_fused(int precision, int rows, int ntiles, const int* tile_species, const int* tile_row,
+                  const fennol_mlp_weights* w, const void* x, const void* x_lo, float* e_rows, float* dx,
+                  void* ws, size_t ws_bytes, cudaStream_t st);

@@ -1,0 +1,603 @@
+// Fused, persistent species MLP on tcgen05 (sm_100a): forward + input gradient
+// of FullyConnectedNet (src/fennol/models/misc/nets.py:13-102) inside
+// SpeciesIndexNet (:301-426), with the ensemble mean, in one launch.
+//
+// One CTA per SM loops over 128-row tiles (one species each) and, for every
+// model of the ensemble, runs the six GEMMs of the layer chain
+//     L1 X.W1  L2 H1.W2  L3 H2.W3 (+ energy head)  B3 G3.W3^T  B2 G2.W2^T  B1 G1.W1^T
+// keeping the activations on chip:
+//   * warp 0 (one thread) streams the AEV tile and W1^T through a 2-stage TMA
+//     ring that aliases the activation buffer, and all other weights through a
+//     3-stage TMA ring;
+//   * warp 1 owns the 512 TMEM columns (two 256-column FP32 accumulators used
+//     alternately) and one thread issues tcgen05.mma / tcgen05.commit;
+//   * warps 2-9 are the epilogue: they read an accumulator (tcgen05.ld, one
+//     row per thread, two warps per lane quarter), apply bias + CELU, the energy
+//     head, or CELU' masks, and write the next A operand as BF16 hi + lo pairs
+//     straight into shared memory in the 128-byte-swizzled K-major layout the
+//     MMA descriptors expect (fence.proxy.async before the MMA reads it).
+// CELU' of layers 1-2 (needed by the backward) goes to a per-CTA scratch in
+// global memory that stays L2 resident.  The ensemble is processed model by
+// model inside the CTA, so the per-row energy and dE/dAEV sums are
+// deterministic.  Every wait is bounded (2 s); a timeout sets the error word,
+// raises a shared abort flag that ends all roles, and the CTA frees its TMEM.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include "mlp_common.cuh"
+#include "umma.cuh"
+
+using namespace fnl;
+using namespace fnl::umma;
+
+namespace {
+
+constexpr int kThreads = 320;
+constexpr int kEpiThreads = 256;
+constexpr int BM = 128, BK = 64;
+constexpr uint32_t kAtom = BM * BK * 2;           // one 128 x 64 BF16 K-atom: 16 KB
+constexpr uint32_t kActHalf = 4 * kAtom;          // up to K = 256 per hi (or lo) operand
+constexpr uint32_t kActBytes = 2 * kActHalf;      // 128 KB
+constexpr int kWStages = 3;
+constexpr uint32_t kWStage = 256 * BK * 2;        // 32 KB
+constexpr uint32_t kXStage = kActBytes / 2;       // 64 KB: A hi | A lo | B (<= 256 rows)
+constexpr uint32_t kSmemMain = kActBytes + kWStages * kWStage;  // 224 KB
+constexpr uint64_t kTimeoutNs = 2000000000ull;
+
+struct FusedParams {
+  int ntiles, n_models, n_species;
+  const int* tile_species;
+  const int* tile_row;
+  int d0, d1, d2, d3;
+  int a_lo;
+  float alpha, inv_models;
+  const float* b1;
+  const float* b2;
+  const float* b3;
+  const float* w4;
+  const float* b4;
+  float* e_rows;
+  float* dx;
+  float* dc;  // [gridDim.x][128][d1 + d2]
+  int* err;
+};
+
+struct Maps {
+  CUtensorMap x, xlo, w1t, w2t, w3t, w3, w2, w1;
+};
+
+struct Bars {
+  uint64_t x_full[2], x_empty[2], w_full[kWStages], w_empty[kWStages];
+  uint64_t acc_full[2], acc_free[2], act_ready, act_free, done;
+  uint32_t tmem_slot;
+  int abort_flag;
+};
+
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ float celu_fast(float x, float alpha) {
+  return x > 0.f ? x : alpha * (__expf(x / alpha) - 1.f);
+}
+__device__ __forceinline__ float dcelu_z(float z, float alpha) { return z > 0.f ? 1.f : __expf(z / alpha); }
+
+// Bounded wait that also gives up when another role has aborted.
+__device__ __forceinline__ bool wait_bar(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* err) {
+  if (mbar_test(bar, parity)) return true;
+  const uint64_t deadline = globaltimer() + kTimeoutNs;
+  uint32_t spins = 0;
+  while (true) {
+    if (mbar_test(bar, parity)) return true;
+    if ((++spins & 63u) == 0) {
+      if (*abort_flag) return false;
+      if (globaltimer() > deadline) {
+        *abort_flag = 1;
+        atomicExch(err, 1);
+        return false;
+      }
+      __nanosleep(32);
+    }
+  }
+}
+
+// Write 32 consecutive columns [n, n+32) of row r as BF16 hi (+ lo) into the
+// swizzled K-major activation buffer.
+__device__ __forceinline__ void act_store(uint8_t* act, int r, int n, const float* v, bool with_lo) {
+  uint32_t h[16], l[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    __nv_bfloat16 a = __float2bfloat16_rn(v[2 * k]), b = __float2bfloat16_rn(v[2 * k + 1]);
+    h[k] = (uint32_t)__bfloat16_as_ushort(a) | ((uint32_t)__bfloat16_as_ushort(b) << 16);
+    __nv_bfloat16 c = __float2bfloat16_rn(v[2 * k] - __bfloat162float(a));
+    __nv_bfloat16 d = __float2bfloat16_rn(v[2 * k + 1] - __bfloat162float(b));
+    l[k] = (uint32_t)__bfloat16_as_ushort(c) | ((uint32_t)__bfloat16_as_ushort(d) << 16);
+  }
+  const int atom = n >> 6;
+  const int j0 = (n & 63) >> 3;
+  const uint32_t rowoff = (uint32_t)(r >> 3) * 1024u + (uint32_t)(r & 7) * 128u;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const uint32_t off = rowoff + (uint32_t)(((j0 + q) ^ (r & 7)) << 4);
+    *reinterpret_cast<uint4*>(act + atom * kAtom + off) = make_uint4(h[4 * q], h[4 * q + 1], h[4 * q + 2], h[4 * q + 3]);
+    if (with_lo)
+      *reinterpret_cast<uint4*>(act + kActHalf + atom * kAtom + off) =
+          make_uint4(l[4 * q], l[4 * q + 1], l[4 * q + 2], l[4 * q + 3]);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant__ Maps maps, const FusedParams p) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint8_t* act = smem;                     // 128 KB, aliased by the L1 ring
+  uint8_t* wring = smem + kActBytes;       // 3 x 32 KB
+  Bars* bars = reinterpret_cast<Bars*>(smem + kSmemMain);
+  volatile int* abort_flag = &bars->abort_flag;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int M = p.n_models;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < 2; ++s) {
+      mbar_init(&bars->x_full[s], 1);
+      mbar_init(&bars->x_empty[s], 1);
+      mbar_init(&bars->acc_full[s], 1);
+      mbar_init(&bars->acc_free[s], kEpiThreads / 32);
+    }
+    for (int s = 0; s < kWStages; ++s) {
+      mbar_init(&bars->w_full[s], 1);
+      mbar_init(&bars->w_empty[s], 1);
+    }
+    mbar_init(&bars->act_ready, kEpiThreads);
+    mbar_init(&bars->act_free, 1);
+    mbar_init(&bars->done, 1);
+    bars->abort_flag = 0;
+    fence_barrier_init();
+  }
+  if (warp == 1) tmem_alloc(&bars->tmem_slot, 512);
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = bars->tmem_slot;
+
+  const uint32_t x_tx = kAtom * (1 + p.a_lo) + (uint32_t)p.d1 * BK * 2;
+
+  if (warp == 0) {
+    // ------------------------------------------------------------------ TMA producer
+    if (lane == 0) {
+      uint32_t xq = 0, wq = 0;
+      int item = 0;
+      bool ok = true;
+      for (int w = blockIdx.x; w < p.ntiles && ok; w += gridDim.x) {
+        const int row0 = p.tile_row[w];
+        const int sp = p.tile_species[w];
+        for (int m = 0; m < M && ok; ++m, ++item) {
+          const int g = m * p.n_species + sp;
+          if (item > 0 && !(ok = wait_bar(&bars->act_free, (item - 1) & 1, abort_flag, p.err))) break;
+          for (int kc = 0; kc < p.d0 / BK; ++kc, ++xq) {
+            const int s = xq & 1;
+            const uint32_t u = xq >> 1;
+            if (u > 0 && !(ok = wait_bar(&bars->x_empty[s], (u - 1) & 1, abort_flag, p.err))) break;
+            uint8_t* st = act + s * kXStage;
+            mbar_expect_tx(&bars->x_full[s], x_tx);
+            tma_load_2d(&maps.x, &bars->x_full[s], st, kc * BK, row0);
+            if (p.a_lo) tma_load_2d(&maps.xlo, &bars->x_full[s], st + kAtom, kc * BK, row0);
+            tma_load_2d(&maps.w1t, &bars->x_full[s], st + 2 * kAtom, kc * BK, g * p.d1);
+          }
+          if (!ok) break;
+          // weight chunks of the remaining GEMMs, in MMA order
+          const CUtensorMap* wm[5] = {&maps.w2t, &maps.w3t, &maps.w3, &maps.w2, &maps.w1};
+          const int rows_g[5] = {p.d2, p.d3, p.d2, p.d1, p.d0};
+          const int box[5] = {p.d2, p.d3, p.d2, p.d1, 256};
+          const int nk[5] = {p.d1 / BK, p.d2 / BK, p.d3 / BK, p.d2 / BK, p.d1 / BK};
+          const int nchunk[5] = {1, 1, 1, 1, p.d0 / 256};
+          for (int jb = 0; jb < 5 && ok; ++jb) {
+            for (int c = 0; c < nchunk[jb] && ok; ++c) {
+              for (int kc = 0; kc < nk[jb]; ++kc, ++wq) {
+                const int s = wq % kWStages;
+                const uint32_t u = wq / kWStages;
+                if (u > 0 && !(ok = wait_bar(&bars->w_empty[s], (u - 1) & 1, abort_flag, p.err))) break;
+                mbar_expect_tx(&bars->w_full[s], (uint32_t)box[jb] * BK * 2);
+                tma_load_2d(wm[jb], &bars->w_full[s], wring + s * kWStage, kc * BK, g * rows_g[jb] + c * 256);
+              }
+            }
+          }
+        }
+      }
+      // Before the CTA can exit, every issued TMA load must have landed (on an
+      // abort some stages may never be consumed).  Bounded, ignores the abort flag.
+      int dummy = 0;
+      for (uint32_t s = 0; s < 2 && s < xq; ++s) {
+        const uint32_t last = xq - 1 - ((xq - 1 - s) % 2);
+        wait_bar(&bars->x_full[s], (last >> 1) & 1, &dummy, p.err);
+      }
+      for (uint32_t s = 0; s < (uint32_t)kWStages && s < wq; ++s) {
+        const uint32_t last = wq - 1 - ((wq - 1 - s) % kWStages);
+        wait_bar(&bars->w_full[s], (last / kWStages) & 1, &dummy, p.err);
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      uint32_t xq = 0, wq = 0, act_phase = 0;
+      uint32_t nuse[2] = {0, 0};
+      uint32_t job = 0;
+      bool ok = true;
+      const uint32_t act_hi = smem_u32(act), act_lo = smem_u32(act + kActHalf);
+      auto acquire_acc = [&](uint32_t b) -> bool {
+        if (nuse[b] == 0) return true;
+        return wait_bar(&bars->acc_free[b], (nuse[b] - 1) & 1, abort_flag, p.err);
+      };
+      // one GEMM whose A operand is the activation buffer (K/64 atoms) and B the weight ring
+      auto gemm_act = [&](int n, int k, uint32_t b) -> bool {
+        const uint32_t idesc = idesc_bf16_f32(n);
+        const uint32_t d = tmem + b * 256;
+        for (int kc = 0; kc < k / BK; ++kc, ++wq) {
+          const int s = wq % kWStages;
+          if (!wait_bar(&bars->w_full[s], (wq / kWStages) & 1, abort_flag, p.err)) return false;
+          fence_after_sync();
+          const uint32_t bs = smem_u32(wring + s * kWStage);
+#pragma unroll
+          for (int kk = 0; kk < BK / 16; ++kk) {
+            const uint64_t bd = sdesc_sw128(bs + kk * 32);
+            mma_bf16(d, sdesc_sw128(act_hi + kc * kAtom + kk * 32), bd, idesc, (kc | kk) != 0);
+            if (p.a_lo) mma_bf16(d, sdesc_sw128(act_lo + kc * kAtom + kk * 32), bd, idesc, 1u);
+          }
+          mma_commit(&bars->w_empty[s]);
+        }
+        return true;
+      };
+      for (int w = blockIdx.x; w < p.ntiles && ok; w += gridDim.x) {
+        for (int m = 0; m < M && ok; ++m) {
+          // L1: A and B from the X ring
+          {
+            const uint32_t b = job & 1;
+            if (!(ok = acquire_acc(b))) break;
+            const uint32_t idesc = idesc_bf16_f32(p.d1);
+            const uint32_t d = tmem + b * 256;
+            for (int kc = 0; kc < p.d0 / BK; ++kc, ++xq) {
+              const int s = xq & 1;
+              if (!(ok = wait_bar(&bars->x_full[s], (xq >> 1) & 1, abort_flag, p.err))) break;
+              fence_after_sync();
+              const uint32_t st = smem_u32(act + s * kXStage);
+#pragma unroll
+              for (int kk = 0; kk < BK / 16; ++kk) {
+                const uint64_t bd = sdesc_sw128(st + 2 * kAtom + kk * 32);
+                mma_bf16(d, sdesc_sw128(st + kk * 32), bd, idesc, (kc | kk) != 0);
+                if (p.a_lo) mma_bf16(d, sdesc_sw128(st + kAtom + kk * 32), bd, idesc, 1u);
+              }
+              mma_commit(&bars->x_empty[s]);
+            }
+            if (!ok) break;
+            mma_commit(&bars->acc_full[b]);
+            ++nuse[b];
+            ++job;
+          }
+          // L2, L3, B3, B2: A from the activation buffer written by the epilogue
+          const int ns[4] = {p.d2, p.d3, p.d2, p.d1};
+          const int ks[4] = {p.d1, p.d2, p.d3, p.d2};
+          for (int jb = 0; jb < 4 && ok; ++jb) {
+            if (!(ok = wait_bar(&bars->act_ready, act_phase & 1, abort_flag, p.err))) break;
+            ++act_phase;
+            fence_after_sync();
+            const uint32_t b = job & 1;
+            if (!(ok = acquire_acc(b))) break;
+            if (!(ok = gemm_act(ns[jb], ks[jb], b))) break;
+            mma_commit(&bars->acc_full[b]);
+            ++nuse[b];
+            ++job;
+          }
+          if (!ok) break;
+          // B1: dX chunks of 256 columns, A = G1
+          if (!(ok = wait_bar(&bars->act_ready, act_phase & 1, abort_flag, p.err))) break;
+          ++act_phase;
+          fence_after_sync();
+          for (int c = 0; c < p.d0 / 256 && ok; ++c) {
+            const uint32_t b = job & 1;
+            if (!(ok = acquire_acc(b))) break;
+            if (!(ok = gemm_act(256, p.d1, b))) break;
+            mma_commit(&bars->acc_full[b]);
+            ++nuse[b];
+            ++job;
+          }
+          if (!ok) break;
+          mma_commit(&bars->act_free);
+        }
+      }
+      // all issued MMAs complete before TMEM is released
+      mma_commit(&bars->done);
+      wait_bar(&bars->done, 0, abort_flag, p.err);
+    }
+  } else {
+    // ------------------------------------------------------------------ epilogue
+    const int q = warp & 3;
+    const int half = (warp - 2) >> 2;
+    const int r = 32 * q + lane;
+    const uint32_t lane_base = (uint32_t)(32 * q) << 16;
+    uint32_t nuse[2] = {0, 0};
+    uint32_t job = 0;
+    bool ok = true;
+    float* dc = p.dc + (size_t)blockIdx.x * BM * (p.d1 + p.d2) + (size_t)r * (p.d1 + p.d2);
+    const bool with_lo = p.a_lo != 0;
+    auto take_acc = [&](uint32_t b) -> bool {
+      bool ready = __all_sync(0xffffffffu, wait_bar(&bars->acc_full[b], nuse[b] & 1, abort_flag, p.err));
+      if (ready) fence_after_sync();
+      return ready;
+    };
+    auto release_acc = [&](uint32_t b) {
+      fence_before_sync();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&bars->acc_free[b]);
+      ++nuse[b];
+      ++job;
+    };
+    auto publish_act = [&]() {
+      fence_proxy_async();
+      mbar_arrive(&bars->act_ready);
+    };
+    for (int w = blockIdx.x; w < p.ntiles && ok; w += gridDim.x) {
+      const int row = p.tile_row[w] + r;
+      const int sp = p.tile_species[w];
+      for (int m = 0; m < M && ok; ++m) {
+        const int g = m * p.n_species + sp;
+        // E1: H1 = celu(Z1 + b1) -> act; celu'(z1) -> dc[0:d1]
+        {
+          const uint32_t b = job & 1;
+          if (!(ok = take_acc(b))) break;
+          const float* bias = p.b1 + (size_t)g * p.d1;
+          for (int cc = half; cc < p.d1 / 32; cc += 2) {
+            float v[32];
+            tmem_ld32(tmem + b * 256 + lane_base + cc * 32, v);
+            float4* dco = reinterpret_cast<float4*>(dc + cc * 32);
+#pragma unroll
+            for (int k = 0; k < 32; k += 4) {
+              float z0 = v[k] + __ldg(bias + cc * 32 + k), z1 = v[k + 1] + __ldg(bias + cc * 32 + k + 1);
+              float z2 = v[k + 2] + __ldg(bias + cc * 32 + k + 2), z3 = v[k + 3] + __ldg(bias + cc * 32 + k + 3);
+              dco[k / 4] = make_float4(dcelu_z(z0, p.alpha), dcelu_z(z1, p.alpha), dcelu_z(z2, p.alpha),
+                                       dcelu_z(z3, p.alpha));
+              v[k] = celu_fast(z0, p.alpha);
+              v[k + 1] = celu_fast(z1, p.alpha);
+              v[k + 2] = celu_fast(z2, p.alpha);
+              v[k + 3] = celu_fast(z3, p.alpha);
+            }
+            act_store(act, r, cc * 32, v, with_lo);
+          }
+          release_acc(b);
+          publish_act();
+        }
+        // E2: H2 = celu(Z2 + b2) -> act; celu'(z2) -> dc[d1:d1+d2]
+        {
+          const uint32_t b = job & 1;
+          if (!(ok = take_acc(b))) break;
+          const float* bias = p.b2 + (size_t)g * p.d2;
+          for (int cc = half; cc < p.d2 / 32; cc += 2) {
+            float v[32];
+            tmem_ld32(tmem + b * 256 + lane_base + cc * 32, v);
+            float4* dco = reinterpret_cast<float4*>(dc + p.d1 + cc * 32);
+#pragma unroll
+            for (int k = 0; k < 32; k += 4) {
+              float z0 = v[k] + __ldg(bias + cc * 32 + k), z1 = v[k + 1] + __ldg(bias + cc * 32 + k + 1);
+              float z2 = v[k + 2] + __ldg(bias + cc * 32 + k + 2), z3 = v[k + 3] + __ldg(bias + cc * 32 + k + 3);
+              dco[k / 4] = make_float4(dcelu_z(z0, p.alpha), dcelu_z(z1, p.alpha), dcelu_z(z2, p.alpha),
+                                       dcelu_z(z3, p.alpha));
+              v[k] = celu_fast(z0, p.alpha);
+              v[k + 1] = celu_fast(z1, p.alpha);
+              v[k + 2] = celu_fast(z2, p.alpha);
+              v[k + 3] = celu_fast(z3, p.alpha);
+            }
+            act_store(act, r, cc * 32, v, with_lo);
+          }
+          release_acc(b);
+          publish_act();
+        }
+        // E3: energy head; G3 = w4 * celu'(z3) -> act.  The column-half-0 warp of
+        // each lane quarter does all columns, so every row's energy sum stays
+        // in one thread (no barrier between warps: an aborting warp can never
+        // leave another waiting).
+        {
+          const uint32_t b = job & 1;
+          if (!(ok = take_acc(b))) break;
+          if (half == 0) {
+            const float* bias = p.b3 + (size_t)g * p.d3;
+            const float* w4 = p.w4 + (size_t)g * p.d3;
+            float e = 0.f;
+            for (int cc = 0; cc < p.d3 / 32; ++cc) {
+              float v[32];
+              tmem_ld32(tmem + b * 256 + lane_base + cc * 32, v);
+#pragma unroll
+              for (int k = 0; k < 32; ++k) {
+                float z = v[k] + __ldg(bias + cc * 32 + k);
+                float wv = __ldg(w4 + cc * 32 + k);
+                e = fmaf(celu_fast(z, p.alpha), wv, e);
+                v[k] = wv * dcelu_z(z, p.alpha);
+              }
+              act_store(act, r, cc * 32, v, with_lo);
+            }
+            e += __ldg(p.b4 + g);
+            const float prev = m == 0 ? 0.f : p.e_rows[row];
+            p.e_rows[row] = prev + e * p.inv_models;
+          }
+          release_acc(b);
+          publish_act();
+        }
+        // E4: G2 = D2 * celu'(z2) -> act
+        {
+          const uint32_t b = job & 1;
+          if (!(ok = take_acc(b))) break;
+          for (int cc = half; cc < p.d2 / 32; cc += 2) {
+            float v[32];
+            tmem_ld32(tmem + b * 256 + lane_base + cc * 32, v);
+            const float4* dci = reinterpret_cast<const float4*>(dc + p.d1 + cc * 32);
+#pragma unroll
+            for (int k = 0; k < 32; k += 4) {
+              float4 dd = dci[k / 4];
+              v[k] *= dd.x;
+              v[k + 1] *= dd.y;
+              v[k + 2] *= dd.z;
+              v[k + 3] *= dd.w;
+            }
+            act_store(act, r, cc * 32, v, with_lo);
+          }
+          release_acc(b);
+          publish_act();
+        }
+        // E5: G1 = D1 * celu'(z1) -> act
+        {
+          const uint32_t b = job & 1;
+          if (!(ok = take_acc(b))) break;
+          for (int cc = half; cc < p.d1 / 32; cc += 2) {
+            float v[32];
+            tmem_ld32(tmem + b * 256 + lane_base + cc * 32, v);
+            const float4* dci = reinterpret_cast<const float4*>(dc + cc * 32);
+#pragma unroll
+            for (int k = 0; k < 32; k += 4) {
+              float4 dd = dci[k / 4];
+              v[k] *= dd.x;
+              v[k + 1] *= dd.y;
+              v[k + 2] *= dd.z;
+              v[k + 3] *= dd.w;
+            }
+            act_store(act, r, cc * 32, v, with_lo);
+          }
+          release_acc(b);
+          publish_act();
+        }
+        // E6: dX chunks
+        for (int c = 0; c < p.d0 / 256 && ok; ++c) {
+          const uint32_t b = job & 1;
+          if (!(ok = take_acc(b))) break;
+          float* out = p.dx + (size_t)row * p.d0 + c * 256;
+          for (int cc = half; cc < 8; cc += 2) {
+            float v[32];
+            tmem_ld32(tmem + b * 256 + lane_base + cc * 32, v);
+            float4* o = reinterpret_cast<float4*>(out + cc * 32);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+              float4 a = make_float4(v[4 * k] * p.inv_models, v[4 * k + 1] * p.inv_models,
+                                     v[4 * k + 2] * p.inv_models, v[4 * k + 3] * p.inv_models);
+              if (m > 0) {
+                float4 pv = o[k];
+                a.x += pv.x;
+                a.y += pv.y;
+                a.z += pv.z;
+                a.w += pv.w;
+              }
+              o[k] = a;
+            }
+          }
+          release_acc(b);
+        }
+      }
+    }
+  }
+  fence_before_sync();
+  __syncthreads();
+  if (warp == 1) {
+    fence_after_sync();
+    tmem_dealloc(tmem, 512);
+  }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* ptr = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+  }
+  return fn;
+}
+
+bool map2d(CUtensorMap* m, const void* base, uint64_t rows, uint64_t cols, uint32_t box_rows) {
+  auto fn = encode_fn();
+  if (!fn || !base) return false;
+  cuuint64_t dims[2] = {cols, rows};
+  cuuint64_t strides[1] = {cols * 2};
+  cuuint32_t box[2] = {(cuuint32_t)BK, box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+  }
+  return n;
+}
+
+}  // namespace
+
+// Shape check: the fused kernel needs every hidden width <= 256 (activation
+// buffer), the input width a multiple of 256 and a BF16 or BF16x2 product.
+bool fnl_mlp_fused_supported(int precision, const fennol_mlp_weights* w) {
+  const int* d = w->dims;
+  if (precision != FENNOL_MLP_BF16 && precision != FENNOL_MLP_BF16X2) return false;
+  if (d[0] % 256 != 0 || d[0] > 4096) return false;
+  for (int l = 1; l < 4; ++l)
+    if (d[l] > 256 || d[l] % 64 != 0) return false;
+  return true;
+}
+
+size_t fnl_mlp_fused_workspace(const fennol_mlp_weights* w) {
+  return 256 + (size_t)sm_count() * BM * (w->dims[1] + w->dims[2]) * sizeof(float);
+}
+
+int fnl_mlp_fused(int precision, int rows, int ntiles, const int* tile_species, const int* tile_row,
+                  const fennol_mlp_weights* w, const void* x, const void* x_lo, float* e_rows, float* dx,
+                  void* ws, size_t ws_bytes, cudaStream_t st) {
+  if (!encode_fn()) return FENNOL_ERR_UNSUPPORTED;
+  if (ws_bytes < fnl_mlp_fused_workspace(w)) return FENNOL_ERR_WORKSPACE;
+  const int* d = w->dims;
+  const int G = w->n_models * w->n_species;
+  const bool alo = precision == FENNOL_MLP_BF16X2;
+  Maps maps;
+  bool ok = map2d(&maps.x, x, rows, d[0], BM) && map2d(&maps.xlo, alo ? x_lo : x, rows, d[0], BM) &&
+            map2d(&maps.w1t, w->wt_hi[0], (uint64_t)G * d[1], d[0], d[1]) &&
+            map2d(&maps.w2t, w->wt_hi[1], (uint64_t)G * d[2], d[1], d[2]) &&
+            map2d(&maps.w3t, w->wt_hi[2], (uint64_t)G * d[3], d[2], d[3]) &&
+            map2d(&maps.w3, w->w_hi[2], (uint64_t)G * d[2], d[3], d[2]) &&
+            map2d(&maps.w2, w->w_hi[1], (uint64_t)G * d[1], d[2], d[1]) &&
+            map2d(&maps.w1, w->w_hi[0], (uint64_t)G * d[0], d[1], 256);
+  if (!ok) return FENNOL_ERR_CUDA;
+  FusedParams p{};
+  p.ntiles = ntiles;
+  p.n_models = w->n_models;
+  p.n_species = w->n_species;
+  p.tile_species = tile_species;
+  p.tile_row = tile_row;
+  p.d0 = d[0];
+  p.d1 = d[1];
+  p.d2 = d[2];
+  p.d3 = d[3];
+  p.a_lo = alo ? 1 : 0;
+  p.alpha = w->celu_alpha;
+  p.inv_models = 1.0f / (float)w->n_models;
+  p.b1 = w->b32[0];
+  p.b2 = w->b32[1];
+  p.b3 = w->b32[2];
+  p.w4 = w->w32[3];
+  p.b4 = w->b32[3];
+  p.e_rows = e_rows;
+  p.dx = dx;
+  p.err = (int*)ws;
+  p.dc = (float*)((char*)ws + 256);
+  const size_t smem = kSmemMain + sizeof(Bars) + 1024;
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(k_mlp_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+      return FENNOL_ERR_CUDA;
+    attr = true;
+  }
+  if (ntiles <= 0) return FENNOL_OK;
+  const int grid = ntiles < sm_count() ? ntiles : sm_count();
+  k_mlp_fused<<<grid, kThreads, smem, st>>>(maps, p);
+  FNL_CHECK_LAUNCH();
+  return FENNOL_OK;
+}

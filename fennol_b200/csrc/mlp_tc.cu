@@ -23,6 +23,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <cstdlib>
 #include <mutex>
 #include <string>
 #include <unordered_map>
@@ -455,15 +456,21 @@ size_t tc_layout(int rows, const fennol_mlp_weights* w, char* base, TcWs* out) {
 }  // namespace
 
 size_t fnl_mlp_tc_workspace(int precision, int rows, int n_models, const fennol_mlp_weights* w) {
-  (void)precision;
   (void)n_models;
-  return tc_layout(rows, w, nullptr, nullptr);
+  size_t a = tc_layout(rows, w, nullptr, nullptr);
+  if (fnl_mlp_fused_supported(precision, w)) {
+    size_t b = fnl_mlp_fused_workspace(w);
+    if (b > a) a = b;
+  }
+  return a;
 }
 
 int fnl_mlp_tc(int precision, int rows, int ntiles, const int* tile_species, const int* tile_row,
                const fennol_mlp_weights* w, const void* x, const void* x_lo, float* e_rows, float* dx, void* ws,
                size_t ws_bytes, cudaStream_t st) {
   if (!encode_fn()) return FENNOL_ERR_UNSUPPORTED;
+  if (fnl_mlp_fused_supported(precision, w) && !getenv("FENNOL_MLP_UNFUSED"))
+    return fnl_mlp_fused(precision, rows, ntiles, tile_species, tile_row, w, x, x_lo, e_rows, dx, ws, ws_bytes, st);
   const int* d = w->dims;
   for (int l = 0; l < 4; ++l)
     if (d[l] > 1024 || (l > 0 && d[l] > 256)) return FENNOL_ERR_UNSUPPORTED;
