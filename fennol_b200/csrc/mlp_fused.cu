@@ -68,34 +68,37 @@ struct Maps {
 
 struct Bars {
   uint64_t x_full[2], x_empty[2], w_full[kWStages], w_empty[kWStages];
-  uint64_t acc_full[2], acc_free[2], act_ready, act_free, done;
+  uint64_t acc_full[2], acc_free[2], act_ready, act_free, done, ex_ready, ex_free;
   uint32_t tmem_slot;
   int abort_flag;
+  float ex[BM];
 };
 
 __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
-__device__ __forceinline__ float celu_fast(float x, float alpha) {
-  return x > 0.f ? x : alpha * (__expf(x / alpha) - 1.f);
+// CELU and its derivative from one exponential: e = exp(z/alpha) for z <= 0,
+// celu = alpha (e - 1), celu' = e; both are z and 1 for z > 0.
+__device__ __forceinline__ void celu_pair(float z, float alpha, float inv_alpha, float& h, float& dh) {
+  const float e = __expf(fminf(z, 0.f) * inv_alpha);
+  h = z > 0.f ? z : alpha * (e - 1.f);
+  dh = z > 0.f ? 1.f : e;
 }
-__device__ __forceinline__ float dcelu_z(float z, float alpha) { return z > 0.f ? 1.f : __expf(z / alpha); }
 
 // Bounded wait that also gives up when another role has aborted.
+// Threads sleep in mbarrier.try_wait (woken when the phase completes) instead
+// of polling, so waiting epilogue warps do not take issue slots from the MMA
+// and TMA threads.
 __device__ __forceinline__ bool wait_bar(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* err) {
-  if (mbar_test(bar, parity)) return true;
+  if (mbar_try(bar, parity, 20000u)) return true;
   const uint64_t deadline = globaltimer() + kTimeoutNs;
-  uint32_t spins = 0;
   while (true) {
-    if (mbar_test(bar, parity)) return true;
-    if ((++spins & 63u) == 0) {
-      if (*abort_flag) return false;
-      if (globaltimer() > deadline) {
-        *abort_flag = 1;
-        atomicExch(err, 1);
-        return false;
-      }
-      __nanosleep(32);
+    if (mbar_try(bar, parity, 20000u)) return true;
+    if (*abort_flag) return false;
+    if (globaltimer() > deadline) {
+      *abort_flag = 1;
+      atomicExch(err, 1);
+      return false;
     }
   }
 }
@@ -149,6 +152,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
     mbar_init(&bars->act_ready, kEpiThreads);
     mbar_init(&bars->act_free, 1);
     mbar_init(&bars->done, 1);
+    mbar_init(&bars->ex_ready, kEpiThreads / 2);
+    mbar_init(&bars->ex_free, kEpiThreads / 2);
     bars->abort_flag = 0;
     fence_barrier_init();
   }
@@ -313,9 +318,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
     const int r = 32 * q + lane;
     const uint32_t lane_base = (uint32_t)(32 * q) << 16;
     uint32_t nuse[2] = {0, 0};
-    uint32_t job = 0;
+    uint32_t job = 0, ex_phase = 0;
     bool ok = true;
-    float* dc = p.dc + (size_t)blockIdx.x * BM * (p.d1 + p.d2) + (size_t)r * (p.d1 + p.d2);
+    // per-CTA CELU' scratch, column-major [d1 + d2][128] so that a warp's 32 rows are contiguous
+    float* dc = p.dc + (size_t)blockIdx.x * BM * (p.d1 + p.d2) + r;
+    const float inv_alpha = 1.0f / p.alpha;
     const bool with_lo = p.a_lo != 0;
     auto take_acc = [&](uint32_t b) -> bool {
       bool ready = __all_sync(0xffffffffu, wait_bar(&bars->acc_full[b], nuse[b] & 1, abort_flag, p.err));
@@ -346,17 +353,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
           for (int cc = half; cc < p.d1 / 32; cc += 2) {
             float v[32];
             tmem_ld32(tmem + b * 256 + lane_base + cc * 32, v);
-            float4* dco = reinterpret_cast<float4*>(dc + cc * 32);
+            float* dco = dc + (size_t)(cc * 32) * BM;
 #pragma unroll
             for (int k = 0; k < 32; k += 4) {
-              float z0 = v[k] + __ldg(bias + cc * 32 + k), z1 = v[k + 1] + __ldg(bias + cc * 32 + k + 1);
-              float z2 = v[k + 2] + __ldg(bias + cc * 32 + k + 2), z3 = v[k + 3] + __ldg(bias + cc * 32 + k + 3);
-              dco[k / 4] = make_float4(dcelu_z(z0, p.alpha), dcelu_z(z1, p.alpha), dcelu_z(z2, p.alpha),
-                                       dcelu_z(z3, p.alpha));
-              v[k] = celu_fast(z0, p.alpha);
-              v[k + 1] = celu_fast(z1, p.alpha);
-              v[k + 2] = celu_fast(z2, p.alpha);
-              v[k + 3] = celu_fast(z3, p.alpha);
+              const float4 bb = __ldg(reinterpret_cast<const float4*>(bias + cc * 32 + k));
+              const float zz[4] = {v[k] + bb.x, v[k + 1] + bb.y, v[k + 2] + bb.z, v[k + 3] + bb.w};
+#pragma unroll
+              for (int u = 0; u < 4; ++u) {
+                float dh;
+                celu_pair(zz[u], p.alpha, inv_alpha, v[k + u], dh);
+                dco[(size_t)(k + u) * BM] = dh;  // column-major: the warp writes 128 contiguous bytes
+              }
             }
             act_store(act, r, cc * 32, v, with_lo);
           }
@@ -371,51 +378,65 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
           for (int cc = half; cc < p.d2 / 32; cc += 2) {
             float v[32];
             tmem_ld32(tmem + b * 256 + lane_base + cc * 32, v);
-            float4* dco = reinterpret_cast<float4*>(dc + p.d1 + cc * 32);
+            float* dco = dc + (size_t)(p.d1 + cc * 32) * BM;
 #pragma unroll
             for (int k = 0; k < 32; k += 4) {
-              float z0 = v[k] + __ldg(bias + cc * 32 + k), z1 = v[k + 1] + __ldg(bias + cc * 32 + k + 1);
-              float z2 = v[k + 2] + __ldg(bias + cc * 32 + k + 2), z3 = v[k + 3] + __ldg(bias + cc * 32 + k + 3);
-              dco[k / 4] = make_float4(dcelu_z(z0, p.alpha), dcelu_z(z1, p.alpha), dcelu_z(z2, p.alpha),
-                                       dcelu_z(z3, p.alpha));
-              v[k] = celu_fast(z0, p.alpha);
-              v[k + 1] = celu_fast(z1, p.alpha);
-              v[k + 2] = celu_fast(z2, p.alpha);
-              v[k + 3] = celu_fast(z3, p.alpha);
+              const float4 bb = __ldg(reinterpret_cast<const float4*>(bias + cc * 32 + k));
+              const float zz[4] = {v[k] + bb.x, v[k + 1] + bb.y, v[k + 2] + bb.z, v[k + 3] + bb.w};
+#pragma unroll
+              for (int u = 0; u < 4; ++u) {
+                float dh;
+                celu_pair(zz[u], p.alpha, inv_alpha, v[k + u], dh);
+                dco[(size_t)(k + u) * BM] = dh;  // column-major: the warp writes 128 contiguous bytes
+              }
             }
             act_store(act, r, cc * 32, v, with_lo);
           }
           release_acc(b);
           publish_act();
         }
-        // E3: energy head; G3 = w4 * celu'(z3) -> act.  The column-half-0 warp of
-        // each lane quarter does all columns, so every row's energy sum stays
-        // in one thread (no barrier between warps: an aborting warp can never
-        // leave another waiting).
+        // E3: energy head; G3 = w4 * celu'(z3) -> act.  Both column halves work;
+        // the half-1 partial energy of each row reaches the half-0 thread through
+        // shared memory guarded by two mbarriers (bounded waits, no CTA barrier).
         {
           const uint32_t b = job & 1;
           if (!(ok = take_acc(b))) break;
-          if (half == 0) {
-            const float* bias = p.b3 + (size_t)g * p.d3;
-            const float* w4 = p.w4 + (size_t)g * p.d3;
-            float e = 0.f;
-            for (int cc = 0; cc < p.d3 / 32; ++cc) {
-              float v[32];
-              tmem_ld32(tmem + b * 256 + lane_base + cc * 32, v);
+          const float* bias = p.b3 + (size_t)g * p.d3;
+          const float* w4 = p.w4 + (size_t)g * p.d3;
+          float e = 0.f;
+          for (int cc = half; cc < p.d3 / 32; cc += 2) {
+            float v[32];
+            tmem_ld32(tmem + b * 256 + lane_base + cc * 32, v);
 #pragma unroll
-              for (int k = 0; k < 32; ++k) {
-                float z = v[k] + __ldg(bias + cc * 32 + k);
-                float wv = __ldg(w4 + cc * 32 + k);
-                e = fmaf(celu_fast(z, p.alpha), wv, e);
-                v[k] = wv * dcelu_z(z, p.alpha);
+            for (int k = 0; k < 32; k += 4) {
+              const float4 bb = __ldg(reinterpret_cast<const float4*>(bias + cc * 32 + k));
+              const float4 ww = __ldg(reinterpret_cast<const float4*>(w4 + cc * 32 + k));
+              const float zz[4] = {v[k] + bb.x, v[k + 1] + bb.y, v[k + 2] + bb.z, v[k + 3] + bb.w};
+              const float wv[4] = {ww.x, ww.y, ww.z, ww.w};
+#pragma unroll
+              for (int u = 0; u < 4; ++u) {
+                float h, dh;
+                celu_pair(zz[u], p.alpha, inv_alpha, h, dh);
+                e = fmaf(h, wv[u], e);
+                v[k + u] = wv[u] * dh;
               }
-              act_store(act, r, cc * 32, v, with_lo);
             }
-            e += __ldg(p.b4 + g);
+            act_store(act, r, cc * 32, v, with_lo);
+          }
+          release_acc(b);
+          if (half == 1) {
+            // the previous row energies must have been read before they are overwritten
+            if (ex_phase > 0 && !(ok = wait_bar(&bars->ex_free, (ex_phase - 1) & 1, abort_flag, p.err))) break;
+            bars->ex[r] = e;
+            mbar_arrive(&bars->ex_ready);
+          } else {
+            if (!(ok = wait_bar(&bars->ex_ready, ex_phase & 1, abort_flag, p.err))) break;
+            e += bars->ex[r] + __ldg(p.b4 + g);
+            mbar_arrive(&bars->ex_free);
             const float prev = m == 0 ? 0.f : p.e_rows[row];
             p.e_rows[row] = prev + e * p.inv_models;
           }
-          release_acc(b);
+          ++ex_phase;
           publish_act();
         }
         // E4: G2 = D2 * celu'(z2) -> act
@@ -425,15 +446,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
           for (int cc = half; cc < p.d2 / 32; cc += 2) {
             float v[32];
             tmem_ld32(tmem + b * 256 + lane_base + cc * 32, v);
-            const float4* dci = reinterpret_cast<const float4*>(dc + p.d1 + cc * 32);
+            const float* dci = dc + (size_t)(p.d1 + cc * 32) * BM;
 #pragma unroll
-            for (int k = 0; k < 32; k += 4) {
-              float4 dd = dci[k / 4];
-              v[k] *= dd.x;
-              v[k + 1] *= dd.y;
-              v[k + 2] *= dd.z;
-              v[k + 3] *= dd.w;
-            }
+            for (int k = 0; k < 32; ++k) v[k] *= dci[(size_t)k * BM];
             act_store(act, r, cc * 32, v, with_lo);
           }
           release_acc(b);
@@ -446,15 +461,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
           for (int cc = half; cc < p.d1 / 32; cc += 2) {
             float v[32];
             tmem_ld32(tmem + b * 256 + lane_base + cc * 32, v);
-            const float4* dci = reinterpret_cast<const float4*>(dc + cc * 32);
+            const float* dci = dc + (size_t)(cc * 32) * BM;
 #pragma unroll
-            for (int k = 0; k < 32; k += 4) {
-              float4 dd = dci[k / 4];
-              v[k] *= dd.x;
-              v[k + 1] *= dd.y;
-              v[k + 2] *= dd.z;
-              v[k + 3] *= dd.w;
-            }
+            for (int k = 0; k < 32; ++k) v[k] *= dci[(size_t)k * BM];
             act_store(act, r, cc * 32, v, with_lo);
           }
           release_acc(b);
