@@ -8,7 +8,7 @@
 // keeping the activations on chip:
 //   * warp 0 (one thread) streams the AEV tile and W1^T through a 2-stage TMA
 //     ring that aliases the activation buffer, and all other weights through a
-//     3-stage TMA ring;
+//     2-stage TMA ring;
 //   * warp 1 owns the 512 TMEM columns (two 256-column FP32 accumulators used
 //     alternately) and one thread issues tcgen05.mma / tcgen05.commit;
 //   * warps 2-9 are the epilogue: they read an accumulator (tcgen05.ld, one
@@ -38,10 +38,11 @@ constexpr int BM = 128, BK = 64;
 constexpr uint32_t kAtom = BM * BK * 2;           // one 128 x 64 BF16 K-atom: 16 KB
 constexpr uint32_t kActHalf = 4 * kAtom;          // up to K = 256 per hi (or lo) operand
 constexpr uint32_t kActBytes = 2 * kActHalf;      // 128 KB
-constexpr int kWStages = 3;
+constexpr int kWStages = 2;
 constexpr uint32_t kWStage = 256 * BK * 2;        // 32 KB
 constexpr uint32_t kXStage = kActBytes / 2;       // 64 KB: A hi | A lo | B (<= 256 rows)
-constexpr uint32_t kSmemMain = kActBytes + kWStages * kWStage;  // 224 KB
+constexpr uint32_t kXpose = 8 * 32 * 32 * 4;      // per-epilogue-warp 32x32 transpose tiles: 32 KB
+constexpr uint32_t kSmemMain = kActBytes + kWStages * kWStage + kXpose;  // 224 KB
 constexpr uint64_t kTimeoutNs = 2000000000ull;
 
 struct FusedParams {
@@ -132,7 +133,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t* act = smem;                     // 128 KB, aliased by the L1 ring
-  uint8_t* wring = smem + kActBytes;       // 3 x 32 KB
+  uint8_t* wring = smem + kActBytes;       // 2 x 32 KB
+  float* xpose = reinterpret_cast<float*>(smem + kActBytes + kWStages * kWStage);
   Bars* bars = reinterpret_cast<Bars*>(smem + kSmemMain);
   volatile int* abort_flag = &bars->abort_flag;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -469,28 +471,28 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
           release_acc(b);
           publish_act();
         }
-        // E6: dX chunks
+        // E6: dX chunks.  Each 32 x 32 block (32 rows of this warp, 32 columns)
+        // is transposed through a swizzled shared-memory tile so that every
+        // global store writes 128 contiguous bytes of one row.
         for (int c = 0; c < p.d0 / 256 && ok; ++c) {
           const uint32_t b = job & 1;
           if (!(ok = take_acc(b))) break;
-          float* out = p.dx + (size_t)row * p.d0 + c * 256;
+          float* tile = xpose + (warp - 2) * 32 * 32;
           for (int cc = half; cc < 8; cc += 2) {
             float v[32];
             tmem_ld32(tmem + b * 256 + lane_base + cc * 32, v);
-            float4* o = reinterpret_cast<float4*>(out + cc * 32);
 #pragma unroll
-            for (int k = 0; k < 8; ++k) {
-              float4 a = make_float4(v[4 * k] * p.inv_models, v[4 * k + 1] * p.inv_models,
-                                     v[4 * k + 2] * p.inv_models, v[4 * k + 3] * p.inv_models);
-              if (m > 0) {
-                float4 pv = o[k];
-                a.x += pv.x;
-                a.y += pv.y;
-                a.z += pv.z;
-                a.w += pv.w;
-              }
-              o[k] = a;
+            for (int k = 0; k < 32; ++k) tile[lane * 32 + (k ^ lane)] = v[k];
+            __syncwarp();
+            const int col = c * 256 + cc * 32 + lane;
+            const int row_base = p.tile_row[w] + 32 * q;
+#pragma unroll 8
+            for (int rr = 0; rr < 32; ++rr) {
+              const float val = tile[rr * 32 + (lane ^ rr)] * p.inv_models;
+              float* o = p.dx + (size_t)(row_base + rr) * p.d0 + col;
+              *o = m > 0 ? *o + val : val;
             }
+            __syncwarp();
           }
           release_acc(b);
         }
