@@ -162,8 +162,9 @@ __device__ __forceinline__ float exp2f_approx_pos(float x) {
 __device__ __forceinline__ float zeta_pow(float x, int n, float f) {
   if (x <= 0.f) return 0.f;
   float r = 1.f, b = x;
-  for (int e = n; e > 0; e >>= 1) {
-    if (e & 1) r *= b;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {  // n < 64
+    r = ((n >> k) & 1) ? r * b : r;
     b *= b;
   }
   return f != 0.f ? r * exp2f_approx_pos(f * __log2f(x)) : r;
@@ -421,12 +422,14 @@ k_aev_forward(const float4* __restrict__ xyzs, int n, const int* __restrict__ at
 // --------------------------------------------------------------------------------
 // Adjoint: dE/dAEV -> forces.
 // --------------------------------------------------------------------------------
+constexpr int kMaxBlk = kMaxP;  // species-pair blocks of one centre atom
+
 __host__ __device__ __forceinline__ size_t bwd_bytes(int S, int RD, int cap) {
-  return (stage_bytes(cap) + (size_t)cap * 12 + (size_t)S * (RD + 1) * 4 + 15) / 16 * 16;
+  return (stage_bytes(cap) + (size_t)cap * 12 + (size_t)S * (RD + 1) * 4 + (2 * kMaxBlk + 2) * 4 + 15) / 16 * 16;
 }
 
 template <int RD, int AD, int AS>
-__global__ void __launch_bounds__(kAevWarps * 32, 3)
+__global__ void __launch_bounds__(kAevWarps * 32, 4)
 k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ atom_sys,
                const float* __restrict__ sys_cell, const int* __restrict__ nbr_j,
                const unsigned* __restrict__ nbr_shift, const int* __restrict__ nbr_count, int cap,
@@ -443,6 +446,7 @@ k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ a
   float* gys = gxs + cap;
   float* gzs = gys + cap;
   float* gr = gzs + cap;                                              // [S][RD+1]
+  int* blkw = (int*)(gr + S * (RD + 1));                              // block table
 
   const float* g = daev + (size_t)atom_row[i] * ld;
   const int FR = S * RD;
@@ -484,83 +488,101 @@ k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ a
   }
   __syncwarp();
 
-  // ---- angular: present species-pair blocks, lane per triplet
+  // ---- angular: the triplets of all present species-pair blocks are packed
+  // into consecutive warp rounds (lane per triplet); each lane reads the
+  // dE/dAEV row of its own pair block.
   const float zeta = K.zeta, c_ang = K.c_ang, eta_a = K.eta_a;
-  const unsigned present = __ballot_sync(0xffffffffu, lane < S && cnt_a > 0);
-  for (unsigned m1 = present; m1; m1 &= m1 - 1) {
-    const int s1 = __ffs(m1) - 1;
-    const int n1 = min(__shfl_sync(0xffffffffu, cnt_a, s1), kCapA);
-    const int o1 = __shfl_sync(0xffffffffu, off_a, s1);
-    for (unsigned m2 = m1; m2; m2 &= m2 - 1) {
-      const int s2 = __ffs(m2) - 1;
-      const int n2 = min(__shfl_sync(0xffffffffu, cnt_a, s2), kCapA);
-      const int o2 = __shfl_sync(0xffffffffu, off_a, s2);
-      int T = s1 == s2 ? n1 * (n1 - 1) / 2 : n1 * n2;
-      if (o1 + n1 > kCapA || o2 + n2 > kCapA) T = 0;
-      if (T == 0) continue;
-      const int p = triu_pair(s1, s2, S);
-      float G[32];
-      const float* gp = g + FR + p * 32;
-#pragma unroll
-      for (int k = 0; k < 32; ++k) G[k] = __ldg(gp + k);
-      for (int t = lane; t < T; t += 32) {
-        int a, b;
-        if (s1 == s2) {
-          diag_ab(t, n1, a, b);
-          a += o1;
-          b += o1;
-        } else {
-          const int aa = t % n1, dd = t / n1;
-          a = o1 + aa;
-          b = o2 + (aa + dd) % n2;
-        }
-        const float4 ua = st.au[a], ub = st.au[b];
-        const float2 fa2 = st.af[a], fb2 = st.af[b];
-        const float cosang = ua.x * ub.x + ua.y * ub.y + ua.z * ub.z;
-        const float ct = 0.95f * cosang;
-        const float stt = sqrtf(fmaxf(1.0f - ct * ct, 1e-12f));
-        float A[AS], Ap[AS];
-#pragma unroll
-        for (int z = 0; z < AS; ++z) {
-          float cz = ct * K.cosz[z] + stt * K.sinz[z];
-          float sz = stt * K.cosz[z] - ct * K.sinz[z];
-          float bs = fmaxf(1.0f + cz, 0.f);
-          float pw1 = zeta_pow(bs, K.zeta1_n, K.zeta1_f);
-          A[z] = pw1 * bs;
-          Ap[z] = -zeta * pw1 * sz;
-        }
-        const float dm = 0.5f * (ua.w + ub.w);
-        float Q = 0.f, Th = 0.f, Dm = 0.f;
-#pragma unroll
-        for (int r = 0; r < AD; ++r) {
-          float x = dm - K.shift_a[r];
-          float Bv = fexp(-eta_a * x * x);
-          float GA = 0.f, GAp = 0.f;
-#pragma unroll
-          for (int z = 0; z < AS; ++z) {
-            GA = fmaf(G[r * AS + z], A[z], GA);
-            GAp = fmaf(G[r * AS + z], Ap[z], GAp);
-          }
-          Q = fmaf(GA, Bv, Q);
-          Th = fmaf(GAp, Bv, Th);
-          Dm = fmaf(GA, -2.f * eta_a * x * Bv, Dm);
-        }
-        const float fa = fa2.x, fb = fb2.x;
-        const float cfab = c_ang * fa * fb;
-        const float dEddm = cfab * Dm;
-        const float dEdda = 0.5f * dEddm + c_ang * fb * Q * fa2.y;
-        const float dEddb = 0.5f * dEddm + c_ang * fa * Q * fb2.y;
-        const float dEdc = cfab * Th * (-0.95f / stt);
-        const float ia = dEdc / ua.w, ib = dEdc / ub.w;
-        const int sa_ = st.aslot[a], sb_ = st.aslot[b];
-        atomicAdd(gxs + sa_, dEdda * ua.x + ia * (ub.x - cosang * ua.x));
-        atomicAdd(gys + sa_, dEdda * ua.y + ia * (ub.y - cosang * ua.y));
-        atomicAdd(gzs + sa_, dEdda * ua.z + ia * (ub.z - cosang * ua.z));
-        atomicAdd(gxs + sb_, dEddb * ub.x + ib * (ua.x - cosang * ub.x));
-        atomicAdd(gys + sb_, dEddb * ub.y + ib * (ua.y - cosang * ub.y));
-        atomicAdd(gzs + sb_, dEddb * ub.z + ib * (ua.z - cosang * ub.z));
+  int* blk_cum = blkw;               // [kMaxBlk + 2]: first triplet of each block, end, count
+  int* blk_ss = blkw + kMaxBlk + 2;  // [kMaxBlk] s1 | s2 << 8
+  if (lane == 0) {
+    int nb = 0, tot = 0;
+    for (int s1 = 0; s1 < S; ++s1) {
+      const int n1 = min(st.cntw[S + s1], kCapA);
+      const int o1 = st.cntw[3 * S + s1] - st.cntw[S + s1];  // running offset ended at off + count
+      if (n1 == 0) continue;
+      for (int s2 = s1; s2 < S; ++s2) {
+        const int n2 = min(st.cntw[S + s2], kCapA);
+        const int o2 = st.cntw[3 * S + s2] - st.cntw[S + s2];
+        int T = s1 == s2 ? n1 * (n1 - 1) / 2 : n1 * n2;
+        if (o1 + n1 > kCapA || o2 + n2 > kCapA) T = 0;
+        if (T == 0) continue;
+        blk_cum[nb] = tot;
+        blk_ss[nb] = s1 | (s2 << 8);
+        tot += T;
+        ++nb;
       }
     }
+    blk_cum[nb] = tot;
+    blk_cum[kMaxBlk + 1] = nb;
+  }
+  __syncwarp();
+  const int nblk = blk_cum[kMaxBlk + 1];
+  const int Ttot = blk_cum[nblk];
+  for (int t = lane; t < Ttot; t += 32) {
+    int k = 0;
+    while (k + 1 < nblk && blk_cum[k + 1] <= t) ++k;
+    const int s1 = blk_ss[k] & 0xFF, s2 = blk_ss[k] >> 8;
+    const int tl = t - blk_cum[k];
+    const int n1 = min(st.cntw[S + s1], kCapA), n2 = min(st.cntw[S + s2], kCapA);
+    const int o1 = st.cntw[3 * S + s1] - st.cntw[S + s1], o2 = st.cntw[3 * S + s2] - st.cntw[S + s2];
+    int a, b;
+    if (s1 == s2) {
+      diag_ab(tl, n1, a, b);
+      a += o1;
+      b += o1;
+    } else {
+      const int aa = tl % n1, dd = tl / n1;
+      a = o1 + aa;
+      b = o2 + (aa + dd) % n2;
+    }
+    const int p = triu_pair(s1, s2, S);
+    const float* gp = g + FR + p * 32;
+    const float4 ua = st.au[a], ub = st.au[b];
+    const float2 fa2 = st.af[a], fb2 = st.af[b];
+    const float cosang = ua.x * ub.x + ua.y * ub.y + ua.z * ub.z;
+    const float ct = 0.95f * cosang;
+    const float stt = sqrtf(fmaxf(1.0f - ct * ct, 1e-12f));
+    float A[AS], Ap[AS];
+#pragma unroll
+    for (int z = 0; z < AS; ++z) {
+      float cz = ct * K.cosz[z] + stt * K.sinz[z];
+      float sz = stt * K.cosz[z] - ct * K.sinz[z];
+      float bs = fmaxf(1.0f + cz, 0.f);
+      float pw1 = zeta_pow(bs, K.zeta1_n, K.zeta1_f);
+      A[z] = pw1 * bs;
+      Ap[z] = -zeta * pw1 * sz;
+    }
+    const float dm = 0.5f * (ua.w + ub.w);
+    float Q = 0.f, Th = 0.f, Dm = 0.f;
+#pragma unroll
+    for (int r = 0; r < AD; ++r) {
+      float x = dm - K.shift_a[r];
+      float Bv = fexp(-eta_a * x * x);
+      float GA = 0.f, GAp = 0.f;
+#pragma unroll
+      for (int z = 0; z < AS; ++z) {
+        const float gv = __ldg(gp + r * AS + z);
+        GA = fmaf(gv, A[z], GA);
+        GAp = fmaf(gv, Ap[z], GAp);
+      }
+      Q = fmaf(GA, Bv, Q);
+      Th = fmaf(GAp, Bv, Th);
+      Dm = fmaf(GA, -2.f * eta_a * x * Bv, Dm);
+    }
+    const float fa = fa2.x, fb = fb2.x;
+    const float cfab = c_ang * fa * fb;
+    const float dEddm = cfab * Dm;
+    const float dEdda = 0.5f * dEddm + c_ang * fb * Q * fa2.y;
+    const float dEddb = 0.5f * dEddm + c_ang * fa * Q * fb2.y;
+    const float dEdc = cfab * Th * (-0.95f / stt);
+    const float ia = dEdc / ua.w, ib = dEdc / ub.w;
+    const int sa_ = st.aslot[a], sb_ = st.aslot[b];
+    atomicAdd(gxs + sa_, dEdda * ua.x + ia * (ub.x - cosang * ua.x));
+    atomicAdd(gys + sa_, dEdda * ua.y + ia * (ub.y - cosang * ua.y));
+    atomicAdd(gzs + sa_, dEdda * ua.z + ia * (ub.z - cosang * ua.z));
+    atomicAdd(gxs + sb_, dEddb * ub.x + ib * (ua.x - cosang * ub.x));
+    atomicAdd(gys + sb_, dEddb * ub.y + ib * (ua.y - cosang * ub.y));
+    atomicAdd(gzs + sb_, dEddb * ub.z + ib * (ua.z - cosang * ub.z));
   }
   __syncwarp();
 
