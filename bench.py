@@ -247,6 +247,64 @@ def cpu_baseline(box, n_models, samples=1):
                        f"float32, {sec:.2f} s each")}
 
 
+def ensemble_98k(device, steps, warmup, flush):
+    """The 98,304-atom water box with the 8-model ensemble: BF16 tensor-core
+    form against the float32 CUDA-core form, same MD step, same timing rules."""
+    import torch
+
+    w = WORKLOADS["water98k"]
+    hbm, tf_burst, tf_sust, src = measured_peaks()
+    out = {"workload": w["desc"], "atoms": 0, "models": w["n_models"]}
+    for precision in ("bf16x2", "fp32"):
+        box, pot, eng = make_engine("water98k", precision, device)
+        ms = time_steps(eng, steps, warmup, flush)
+        mlp_ms = time_mlp(pot, eng, 5)
+        flops = MLP_FLOP_PER_ATOM * box.natoms * w["n_models"]
+        out["atoms"] = box.natoms
+        out[precision] = {"value": box.natoms / (float(ms.mean()) * 1e-3), "unit": "atom-steps/s",
+                          "ms_per_step": float(ms.mean()), "mlp_ms_per_launch": mlp_ms,
+                          "mlp_tflops": flops / (mlp_ms * 1e-3) / 1e12,
+                          "mlp_frac_of_peak": flops / (mlp_ms * 1e-3) / 1e12 / tf_sust,
+                          "peak": f"{src} bf16 sustained {tf_sust} TFLOP/s"}
+        del eng, pot
+        torch.cuda.empty_cache()
+    out["speedup_vs_fp32_form"] = out["bf16x2"]["value"] / out["fp32"]["value"]
+    return out
+
+
+def serving_run(device, n_requests=1000, rate_hz=2000.0, seed=0):
+    """Poisson stream through the continuous-batching loop (real time):
+    throughput of the energy/force work done and p50/p99 request latency."""
+    from fennol_b200.params import MD_OUTPUT_SCALE
+    from fennol_b200.potential import ANIPotential
+    from fennol_b200.serving import (ServingEngine, atom_steps, latency_percentiles,
+                                     serve_requests_from_stream)
+    from fennol_b200.systems import request_stream
+
+    pot = ANIPotential(precision="bf16x2", device=device, seed=0, output_scale=MD_OUTPUT_SCALE,
+                       bf16_weights=True)
+    stream = request_stream(n_requests, rate_hz=rate_hz, seed=seed, md_steps=100, pool_size=48)
+    warm = serve_requests_from_stream(request_stream(24, rate_hz=rate_hz, seed=seed + 1, md_steps=10,
+                                                     pool_size=8))
+    eng = ServingEngine(pot, hbm_budget_gb=120.0, segment_steps=10)
+    eng.run(warm, realtime=False)
+    reqs = serve_requests_from_stream(stream)
+    t0 = time.perf_counter()
+    res = eng.run(reqs, realtime=True)
+    wall = time.perf_counter() - t0
+    work = atom_steps(res, {q.rid: q for q in reqs})
+    lat = latency_percentiles(res)
+    n_md = sum(q.kind == "md" for q in reqs)
+    return {"value": work / wall, "unit": "atom-steps/s", "wall_s": wall,
+            "requests": len(reqs), "md_requests": n_md,
+            "atoms_mean": float(np.mean([q.natoms for q in reqs])),
+            "latency_ms": {"p50": lat["p50_ms"], "p99": lat["p99_ms"], "mean": lat["mean_ms"]},
+            "stream": (f"Poisson {rate_hz:.0f} req/s, atoms log-uniform 8-5000 (chains and water "
+                       "boxes, 48 pre-generated systems), 70% single-point E+F, 30% 100-step "
+                       "Langevin MD continuations at dt 0.5 fs; HBM budget 120 GB"),
+            "captures": eng.md.captures}
+
+
 def run_reference(args):
     """Reference arm: the CPU restatement of the reference algorithm, one
     bounded MD-step sample per timed step, rank 0 only."""
@@ -280,6 +338,8 @@ def main():
     ap.add_argument("--workload", default="water12k", choices=list(WORKLOADS))
     ap.add_argument("--precision", default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--skip-98k", action="store_true", help="skip the 98k-atom 8-model comparison")
+    ap.add_argument("--skip-serving", action="store_true", help="skip the request-stream run")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -367,6 +427,12 @@ def main():
                                                    "rounded to BF16 (same weights in the oracle)")
         del spec
         res["e2e"] = e2e(pot, box, max(5, args.steps // 3), 3)
+        if not args.skip_98k and args.workload != "water98k":
+            del eng, pot
+            torch.cuda.empty_cache()
+            res["ensemble_98k"] = ensemble_98k(device, 5, 3, flush)
+        if not args.skip_serving:
+            res["serving"] = serving_run(device)
         if not args.no_cpu_baseline:
             res["cpu_baseline"] = cpu_baseline(box, w["n_models"])
         print(json.dumps(res), flush=True)

@@ -91,6 +91,7 @@ _SIGNATURES = {
     "fennol_energy_reduce": (I, [P, P, I, P, I, D, P, P, P, SZ, P]),
     "fennol_forces_finalize": (I, [P, I, F, P, P]),
     "fennol_md_step": (I, [I, D, P, P, P, P, D, D, P, ULL, P, P, P, P, P, D, P, P]),
+    "fennol_md_step_systems": (I, [I, I, D, P, P, P, P, D, D, P, P, P, P, P, P, P, P, P, D, P, P]),
     "fennol_md_mark_rebuilt": (I, [I, P, P, P, P]),
     "fennol_md_kinetic": (I, [I, P, P, P, P]),
 }

@@ -345,6 +345,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
     for (int w = blockIdx.x; w < p.ntiles && ok; w += gridDim.x) {
       const int row = p.tile_row[w] + r;
       const int sp = p.tile_species[w];
+      float e_row = 0.f;  // ensemble-mean row energy, accumulated model by model in registers
       for (int m = 0; m < M && ok; ++m) {
         const int g = m * p.n_species + sp;
         // E1: H1 = celu(Z1 + b1) -> act; celu'(z1) -> dc[0:d1]
@@ -435,8 +436,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
             if (!(ok = wait_bar(&bars->ex_ready, ex_phase & 1, abort_flag, p.err))) break;
             e += bars->ex[r] + __ldg(p.b4 + g);
             mbar_arrive(&bars->ex_free);
-            const float prev = m == 0 ? 0.f : p.e_rows[row];
-            p.e_rows[row] = prev + e * p.inv_models;
+            e_row += e * p.inv_models;
+            if (m == M - 1) p.e_rows[row] = e_row;
           }
           ++ex_phase;
           publish_act();
@@ -490,7 +491,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
             for (int rr = 0; rr < 32; ++rr) {
               const float val = tile[rr * 32 + (lane ^ rr)] * p.inv_models;
               float* o = p.dx + (size_t)(row_base + rr) * p.d0 + col;
-              *o = m > 0 ? *o + val : val;
+              // later models add with fire-and-forget reductions (no load on the
+              // critical path); one thread owns each element, so the order of
+              // the sum over models is fixed
+              if (m == 0)
+                *o = val;
+              else
+                atomicAdd(o, val);
             }
             __syncwarp();
           }

@@ -141,15 +141,14 @@ __device__ __forceinline__ void box_muller(unsigned a, unsigned b, double& z0, d
   z1 = r * s;
 }
 
-__global__ void k_md_step(int n, double dt, double* __restrict__ x, double* __restrict__ v,
-                          const double* __restrict__ inv_mass, const float4* __restrict__ f4,
-                          double fscale, double a1, const double* __restrict__ a2,
-                          unsigned long long seed, const unsigned long long* __restrict__ step_counter,
-                          float* __restrict__ coords,
-                          const int* __restrict__ sp, float4* __restrict__ xyzs,
-                          const double* __restrict__ x_ref, double half_skin2, int* rebuild_flag) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+// One BAOAB update of atom i; `key`/`ctr` select its Philox noise block.
+__device__ __forceinline__ void md_update(int i, double dt, double* __restrict__ x, double* __restrict__ v,
+                                          const double* __restrict__ inv_mass, const float4* __restrict__ f4,
+                                          double fscale, double a1, const double* __restrict__ a2,
+                                          unsigned long long key, U4 ctr, float* __restrict__ coords,
+                                          const int* __restrict__ sp, float4* __restrict__ xyzs,
+                                          const double* __restrict__ x_ref, double half_skin2,
+                                          int* rebuild_flag) {
   float4 f = f4[i];
   double im = inv_mass[i];
   double vx = v[3 * i], vy = v[3 * i + 1], vz = v[3 * i + 2];
@@ -165,9 +164,7 @@ __global__ void k_md_step(int n, double dt, double* __restrict__ x, double* __re
   pz += h * vz;
   // O: Langevin
   if (a2) {
-    unsigned long long step = *step_counter;
-    U4 r = philox4x32_10(U4{(unsigned)i, (unsigned)(step & 0xffffffffull), (unsigned)(step >> 32), 0x4C47u},
-                         (unsigned)(seed & 0xffffffffull), (unsigned)(seed >> 32));
+    U4 r = philox4x32_10(ctr, (unsigned)(key & 0xffffffffull), (unsigned)(key >> 32));
     double z0, z1, z2, z3;
     box_muller(r.x, r.y, z0, z1);
     box_muller(r.z, r.w, z2, z3);
@@ -197,6 +194,46 @@ __global__ void k_md_step(int n, double dt, double* __restrict__ x, double* __re
     double dx = px - x_ref[3 * i], dy = py - x_ref[3 * i + 1], dz = pz - x_ref[3 * i + 2];
     if (dx * dx + dy * dy + dz * dz > half_skin2) *rebuild_flag = 1;
   }
+}
+
+__global__ void k_md_step(int n, double dt, double* __restrict__ x, double* __restrict__ v,
+                          const double* __restrict__ inv_mass, const float4* __restrict__ f4,
+                          double fscale, double a1, const double* __restrict__ a2,
+                          unsigned long long seed, const unsigned long long* __restrict__ step_counter,
+                          float* __restrict__ coords,
+                          const int* __restrict__ sp, float4* __restrict__ xyzs,
+                          const double* __restrict__ x_ref, double half_skin2, int* rebuild_flag) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  unsigned long long step = a2 ? *step_counter : 0ull;
+  U4 ctr{(unsigned)i, (unsigned)(step & 0xffffffffull), (unsigned)(step >> 32), 0x4C47u};
+  md_update(i, dt, x, v, inv_mass, f4, fscale, a1, a2, seed, ctr, coords, sp, xyzs, x_ref, half_skin2,
+            rebuild_flag);
+}
+
+// Per-system noise streams: atom i of system b draws from the block keyed by
+// sys_seed[b] at counter (i - sys_start[b], sys_step[b]), so a system's
+// trajectory does not depend on which other systems share the batch.
+__global__ void k_md_step_systems(int n, double dt, double* __restrict__ x, double* __restrict__ v,
+                                  const double* __restrict__ inv_mass, const float4* __restrict__ f4,
+                                  double fscale, double a1, const double* __restrict__ a2,
+                                  const int* __restrict__ atom_sys, const int* __restrict__ sys_start,
+                                  const unsigned long long* __restrict__ sys_seed,
+                                  const unsigned long long* __restrict__ sys_step, float* __restrict__ coords,
+                                  const int* __restrict__ sp, float4* __restrict__ xyzs,
+                                  const double* __restrict__ x_ref, double half_skin2, int* rebuild_flag) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int b = atom_sys[i];
+  const unsigned long long step = sys_step[b];
+  U4 ctr{(unsigned)(i - sys_start[b]), (unsigned)(step & 0xffffffffull), (unsigned)(step >> 32), 0x4C47u};
+  md_update(i, dt, x, v, inv_mass, f4, fscale, a1, a2, sys_seed[b], ctr, coords, sp, xyzs, x_ref,
+            half_skin2, rebuild_flag);
+}
+
+__global__ void k_inc_steps(int nsys, unsigned long long* __restrict__ sys_step) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < nsys) sys_step[b] += 1ull;
 }
 
 __global__ void k_inc_counter(unsigned long long* c) { *c += 1ull; }
@@ -287,6 +324,28 @@ extern "C" int fennol_md_step(int natoms, double dt, double* x, double* v, const
     k_inc_counter<<<1, 1, 0, st>>>(step_counter);
     FNL_CHECK_LAUNCH();
   }
+  return FENNOL_OK;
+}
+
+extern "C" int fennol_md_step_systems(int natoms, int nsys, double dt, double* x, double* v,
+                                      const double* inv_mass, const float* forces4, double force_scale,
+                                      double a1, const double* a2, const int* atom_sys, const int* sys_start,
+                                      const unsigned long long* sys_seed, unsigned long long* sys_step,
+                                      float* coords, const int* species_idx, float* xyzs,
+                                      const double* x_ref, double half_skin, int* rebuild_flag,
+                                      void* stream) {
+  if (natoms < 0 || nsys < 0 || !(dt > 0)) return FENNOL_ERR_INVALID;
+  if (natoms == 0) return FENNOL_OK;
+  if (!x || !v || !inv_mass || !forces4 || !atom_sys || !sys_start || !sys_seed || !sys_step || nsys == 0)
+    return FENNOL_ERR_INVALID;
+  if (xyzs && !species_idx) return FENNOL_ERR_INVALID;
+  cudaStream_t st = (cudaStream_t)stream;
+  k_md_step_systems<<<(natoms + 255) / 256, 256, 0, st>>>(
+      natoms, dt, x, v, inv_mass, (const float4*)forces4, force_scale, a1, a2, atom_sys, sys_start, sys_seed,
+      sys_step, coords, species_idx, (float4*)xyzs, x_ref, half_skin * half_skin, rebuild_flag);
+  FNL_CHECK_LAUNCH();
+  k_inc_steps<<<(nsys + 255) / 256, 256, 0, st>>>(nsys, sys_step);
+  FNL_CHECK_LAUNCH();
   return FENNOL_OK;
 }
 

@@ -29,6 +29,8 @@ from .params import AEVConfig, MLPConfig, Weights, init_weights
 
 HARTREE_TO_KCALMOL = 627.5096080305927
 TILE = 128
+MAX_ROW = 512            # longest neighbour row the AEV kernels stage on chip
+MOLECULE_ROW_GUESS = 96  # first row length for molecules (regrown on overflow)
 
 
 def _ceil(a: int, b: int) -> int:
@@ -135,7 +137,10 @@ class Capacities:
 
 
 class BatchLayout:
-    """Static description of a batch: systems, cells, species-sorted rows."""
+    """Static description of a batch: systems, cells, species-sorted rows.
+
+    ``minimum_image`` is one flag for every periodic system or one per
+    system (minimum image when true, general periodic images otherwise)."""
 
     def __init__(self, species_idx: np.ndarray, natoms: Sequence[int], cells=None,
                  minimum_image: bool = True, device="cuda"):
@@ -165,7 +170,9 @@ class BatchLayout:
                 c32 = np.asarray(c, dtype=np.float32).reshape(3, 3)
                 cell_arr[b] = c32
                 recip_arr[b] = np.linalg.inv(c32).astype(np.float32)
-                mode[b] = _lib.PBC_MINIMUM_IMAGE if minimum_image else _lib.PBC_GENERAL
+                mi = minimum_image[b] if isinstance(minimum_image, (list, tuple, np.ndarray)) \
+                    else minimum_image
+                mode[b] = _lib.PBC_MINIMUM_IMAGE if mi else _lib.PBC_GENERAL
         self.has_pbc = bool((mode != 0).any())
         self.mode_host, self.cell_host, self.recip_host = mode, cell_arr, recip_arr
         # species-sorted rows, segments padded to the 128-row tile
@@ -218,12 +225,14 @@ class BatchLayout:
         for b in range(self.nsys):
             nb = int(self.natoms[b])
             if self.mode_host[b] == 0:
-                best = max(best, nb - 1)
+                # molecules: bounded by the size, and by a dense-liquid count
+                # (overflow regrows the rows)
+                best = max(best, min(nb - 1, MOLECULE_ROW_GUESS))
             else:
                 vol = abs(float(np.linalg.det(self.cell_host[b].astype(np.float64))))
                 est = 4.0 / 3.0 * math.pi * cutoff ** 3 * nb / max(vol, 1e-9)
                 best = max(best, int(est * 1.25) + 16)
-        return min(_ceil(max(best, 8), 8), 1024)
+        return min(_ceil(max(best, 8), 8), MAX_ROW)
 
 
 class GraphBuffers:
@@ -405,8 +414,8 @@ class ANIPotential:
                 capr = int(self.capacity_margin * st[_lib.ST_FILTER_MAXCOUNT]) + self.add_neigh
             if g.skin <= 0:
                 capr = cap
-            if max(cap, capr) > 1024:
-                raise RuntimeError("neighbour rows longer than 1024 are not supported")
+            if max(cap, capr) > MAX_ROW:
+                raise RuntimeError(f"neighbour rows longer than {MAX_ROW} are not supported")
             grow = (_ceil(cap, 8), _ceil(capr, 8))
         return grow
 

@@ -123,18 +123,26 @@ class Request:
 
 def request_stream(n_requests: int, rate_hz: float = 2000.0, seed: int = 0,
                    nmin: int = 8, nmax: int = 5000, md_fraction: float = 0.3,
-                   md_steps: int = 100) -> List[Request]:
+                   md_steps: int = 100, pool_size: Optional[int] = None) -> List[Request]:
     """Poisson arrivals; atom counts log-uniform in [nmin, nmax]; half chains,
-    half periodic water boxes; ``md_fraction`` of requests are MD continuations."""
+    half periodic water boxes; ``md_fraction`` of requests are MD continuations.
+
+    With ``pool_size`` the systems are drawn from that many pre-generated ones
+    (sizes log-uniform as above) instead of one new system per request, which
+    keeps generating long streams fast."""
     rng = np.random.default_rng(seed)
     t = np.cumsum(rng.exponential(1.0 / rate_hz, size=n_requests))
-    out = []
-    for k in range(n_requests):
+
+    def new_system() -> System:
         n = int(round(np.exp(rng.uniform(np.log(nmin), np.log(nmax)))))
         if rng.uniform() < 0.5 or n < 24:
-            sys_ = organic_molecule(n, rng)
-        else:
-            sys_ = water_cluster_box(n, seed=int(rng.integers(1 << 30)))
+            return organic_molecule(n, rng)
+        return water_cluster_box(n, seed=int(rng.integers(1 << 30)))
+
+    pool = [new_system() for _ in range(pool_size)] if pool_size else None
+    out = []
+    for k in range(n_requests):
+        sys_ = pool[int(rng.integers(len(pool)))] if pool else new_system()
         kind = "md" if rng.uniform() < md_fraction else "ef"
         out.append(Request(float(t[k]), sys_, kind, md_steps if kind == "md" else 0))
     return out

@@ -314,6 +314,23 @@ int fennol_md_step(int natoms, double dt, double* x, double* v, const double* in
                    const int* species_idx, float* xyzs, const double* x_ref, double half_skin,
                    int* rebuild_flag, void* stream);
 
+/*
+ * fennol_md_step for a batch of independent systems (no counterpart in the
+ * reference, whose MD driver integrates one system; used by the serving
+ * loop).  Same update; the Langevin noise of atom i in system b = atom_sys[i]
+ * comes from the Philox block keyed by sys_seed[b] at counter
+ * (i - sys_start[b], sys_step[b]), so each system's trajectory is the same
+ * whichever systems share the batch.  sys_step[0..nsys) (device uint64) is
+ * incremented after the step.  Atoms [0, natoms) must belong to systems
+ * [0, nsys).
+ */
+int fennol_md_step_systems(int natoms, int nsys, double dt, double* x, double* v,
+                           const double* inv_mass, const float* forces4, double force_scale,
+                           double a1, const double* a2, const int* atom_sys, const int* sys_start,
+                           const unsigned long long* sys_seed, unsigned long long* sys_step,
+                           float* coords, const int* species_idx, float* xyzs,
+                           const double* x_ref, double half_skin, int* rebuild_flag, void* stream);
+
 /* After a rebuild: x_ref = x and *rebuild_flag = 0 (both device). */
 int fennol_md_mark_rebuilt(int natoms, const double* x, double* x_ref, int* rebuild_flag,
                            void* stream);

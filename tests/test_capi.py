@@ -105,3 +105,22 @@ def test_batch_layout_species_tiles():
     assert lay.mode_host.tolist() == [_lib.PBC_MINIMUM_IMAGE, _lib.PBC_NONE]
     assert lay.plan(5.2)[2] == 27   # 20 A / 5.2 A -> 3 bins per axis
     assert lay.plan(7.0)[2] == 0    # 20 A / 7 A -> 2 bins: all-pairs path
+
+
+def test_serving_host_helpers():
+    import numpy as np
+    from fennol_b200.serving import (ServeRequest, ServeResult, _min_image_ok, atom_steps,
+                                     latency_percentiles, serve_requests_from_stream)
+    from fennol_b200.systems import request_stream
+    assert _min_image_ok(None, 6.2)
+    assert _min_image_ok(np.eye(3) * 12.5, 6.2) and not _min_image_ok(np.eye(3) * 12.3, 6.2)
+    stream = request_stream(6, seed=1, nmax=60, pool_size=3)
+    reqs = serve_requests_from_stream(stream, seed=10)
+    assert [q.seed for q in reqs] == list(range(10, 16))
+    assert all(q.arrival > 0 for q in reqs)
+    res = [ServeResult(q.rid, q.kind, q.natoms, 0.0, None, None, None, 0.0, 0.001 * (k + 1))
+           for k, q in enumerate(reqs)]
+    lat = latency_percentiles(res)
+    assert abs(lat["p50_ms"] - 3.5) < 1e-9
+    want = sum(q.natoms * (1 + (q.md_steps if q.kind == "md" else 0)) for q in reqs)
+    assert atom_steps(res, {q.rid: q for q in reqs}) == want
