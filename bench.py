@@ -113,7 +113,7 @@ def measured_peaks():
         return 6650.0, 1590.0, 1400.0, "fallback"
 
 
-def make_engine(workload, precision, device, seed=0, bf16_weights=True):
+def make_engine(workload, precision, device, seed=0, bf16_weights=True, output_scale=None):
     from fennol_b200.md import MDEngine
     from fennol_b200.potential import ANIPotential
     from fennol_b200.systems import water_box
@@ -123,7 +123,8 @@ def make_engine(workload, precision, device, seed=0, bf16_weights=True):
     w = WORKLOADS[workload]
     box = water_box(w["n_side"], seed=seed)
     pot = ANIPotential(precision=precision, device=device, seed=0, n_models=w["n_models"],
-                       output_scale=MD_OUTPUT_SCALE, bf16_weights=bf16_weights)
+                       output_scale=MD_OUTPUT_SCALE if output_scale is None else output_scale,
+                       bf16_weights=bf16_weights)
     eng = MDEngine(pot, box.coordinates, box.species, box.cell, dt_fs=0.5, thermostat=w["thermostat"],
                    temperature=300.0, gamma_ps=1.0, skin=1.0, trigger="displacement", seed=seed)
     return box, pot, eng
@@ -176,6 +177,72 @@ def time_mlp(pot, eng, reps):
     ev1.record()
     torch.cuda.synchronize()
     return ev0.elapsed_time(ev1) / reps
+
+
+def time_launch(fn, reps):
+    """Average device time (ms) of ``fn``'s launches, after 3 warm-up calls."""
+    import torch
+
+    for _ in range(3):
+        fn()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(reps):
+        fn()
+    ev1.record()
+    torch.cuda.synchronize()
+    return ev0.elapsed_time(ev1) / reps
+
+
+def kernel_times(pot, eng, reps=20):
+    """Device time per launch (ms) of the three large kernels of a step, on
+    the current MD state: AEV forward, species MLP, AEV adjoint."""
+    import torch
+    from fennol_b200._lib import call
+    from fennol_b200.potential import C_ptr, _ptr
+
+    lay, ws, g = eng.layout, eng.ws, eng.graph_buf
+    st = torch.cuda.current_stream().cuda_stream
+    lp = C_ptr(pot.params)
+
+    def aev_fwd():
+        call("fennol_aev_forward", ws.xyzs.data_ptr(), lay.n, lay.t_atom_sys.data_ptr(), lay.t_cell.data_ptr(),
+             g.rad_j.data_ptr(), g.rad_s.data_ptr(), g.rad_n.data_ptr(), g.cap_r, lp, lay.t_atom_row.data_ptr(),
+             ws.aev_kind, ws.x.data_ptr(), _ptr(ws.x_lo), ws.x.shape[1], ws.status.data_ptr(), st)
+
+    def aev_bwd():
+        call("fennol_aev_backward", ws.xyzs.data_ptr(), lay.n, lay.t_atom_sys.data_ptr(), lay.t_cell.data_ptr(),
+             g.rad_j.data_ptr(), g.rad_s.data_ptr(), g.rad_n.data_ptr(), g.cap_r, lp, lay.t_atom_row.data_ptr(),
+             ws.dx.data_ptr(), ws.dx.shape[1], ws.forces4.data_ptr(), ws.status.data_ptr(), st)
+
+    out = {"aev_forward": time_launch(aev_fwd, reps), "mlp": time_mlp(pot, eng, reps),
+           "aev_backward": time_launch(aev_bwd, reps)}
+    ws.forces4.zero_()
+    eng._initial_forces_from_current()
+    mean_nbr = float(g.rad_n[:lay.n].float().mean())
+    return out, mean_nbr
+
+
+def profile_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch of ``kernel`` on ``workload`` recorded by an ncu
+    capture in profiles/ (a line ``traffic_bytes_per_launch <kernel> <workload> <bytes>``)."""
+    d = os.path.join(ROOT, "profiles")
+    try:
+        names = sorted(os.listdir(d))
+    except OSError:
+        return None
+    for name in names:
+        try:
+            with open(os.path.join(d, name)) as f:
+                for line in f:
+                    parts = line.strip().strip("`").split()
+                    if len(parts) == 4 and parts[0] == "traffic_bytes_per_launch" and \
+                            parts[1] == kernel and parts[2] == workload:
+                        return float(parts[3])
+        except OSError:
+            continue
+    return None
 
 
 def accuracy(pot, box):
@@ -272,6 +339,47 @@ def ensemble_98k(device, steps, warmup, flush):
     return out
 
 
+DRIFT_OUTPUT_SCALE = 0.005
+
+
+def nve_drift(device, steps, workload="water98k", every=100):
+    """Total-energy record of an NVE run of the workload (BF16 MLP form,
+    float64 integrator): linear drift and largest excursion per atom.
+
+    The random-weight network has no repulsive core: over thousands of steps
+    its wells gather atoms until one centre has more angular neighbours than
+    the kernels hold.  The drift run therefore scales the last layer by
+    ``DRIFT_OUTPUT_SCALE`` (atomic energies well below kT), and stops early,
+    saying so, if a list limit is hit."""
+    box, pot, eng = make_engine(workload, "bf16x2", device, output_scale=DRIFT_OUTPUT_SCALE)
+    n = box.natoms
+    t_ps, etot = [], []
+    done = 0
+    stopped = None
+    t0 = time.perf_counter()
+    while True:
+        etot.append(eng.potential_energy() + eng.kinetic_energy())
+        t_ps.append(done * eng.dt)
+        if done >= steps:
+            break
+        k = min(every, steps - done)
+        try:
+            eng.run(k, graph_steps=1)
+        except RuntimeError as err:
+            stopped = f"stopped after {done} steps: {err}"
+            break
+        done += k
+    wall = time.perf_counter() - t0
+    e = np.array(etot) / n
+    slope = float(np.polyfit(np.array(t_ps), e, 1)[0]) if len(e) > 2 else 0.0
+    return {"workload": WORKLOADS[workload]["desc"] + f"; last layer x{DRIFT_OUTPUT_SCALE} for this run",
+            "steps": done, "stopped": stopped, "dt_fs": eng.dt * 1000.0,
+            "samples": len(e), "drift_kcalmol_atom_per_ns": slope * 1000.0,
+            "max_abs_dev_kcalmol_atom": float(np.abs(e - e[0]).max()),
+            "e0_kcalmol_atom": float(e[0]), "temperature_end_K": eng.temperature(),
+            "rebuilds": eng.rebuild_count(), "wall_s": wall}
+
+
 def serving_run(device, n_requests=1000, rate_hz=2000.0, seed=0):
     """Poisson stream through the continuous-batching loop (real time):
     throughput of the energy/force work done and p50/p99 request latency."""
@@ -340,6 +448,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-98k", action="store_true", help="skip the 98k-atom 8-model comparison")
     ap.add_argument("--skip-serving", action="store_true", help="skip the request-stream run")
+    ap.add_argument("--nve-drift-steps", type=int, default=0,
+                    help="also record NVE energy drift of the 98k-atom ensemble over this many steps")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -378,9 +488,8 @@ def main():
         ms = time_steps(eng, args.steps, args.warmup, flush)
     total_ms = float(ms.sum())
     if world > 1:
-        t = torch.tensor([total_ms], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t)
+        from fennol_b200.replicas import max_over_ranks
+        total_ms = max_over_ranks(total_ms, device)
         dist.barrier()
     value = world * box.natoms * args.steps / (total_ms * 1e-3)
 
@@ -403,14 +512,42 @@ def main():
            "rebuilds_in_run": eng.rebuild_count()}
     if rank == 0:
         hbm, tf_burst, tf_sust, src = measured_peaks()
-        mlp_ms = time_mlp(pot, eng, 20)
+        kt, mean_nbr = kernel_times(pot, eng)
+        mlp_ms = kt["mlp"]
         flops = MLP_FLOP_PER_ATOM * box.natoms * w["n_models"]
-        achieved = flops / (mlp_ms * 1e-3) / 1e12
-        res["roofline"] = {"bound": "tensor", "kernel": "species MLP (fennol_mlp_energy_grad)",
-                           "achieved": achieved, "peak": tf_burst, "unit": "TFLOP/s",
-                           "frac": achieved / tf_burst, "peak_source": f"{src} bf16 burst",
-                           "algorithmic_flop_per_launch": flops, "ms_per_launch": mlp_ms,
-                           "traffic": None}
+        mlp_tf = flops / (mlp_ms * 1e-3) / 1e12
+        # algorithmic bytes per atom of the adjoint: its dE/dAEV row (float32),
+        # its neighbour row (index + packed shift), its position in and force out
+        bwd_bytes = box.natoms * (1008 * 4 + mean_nbr * 8 + 16 + 16)
+        # forward: neighbour row and position in, AEV row out (BF16 hi + lo or float32)
+        fwd_bytes = box.natoms * (mean_nbr * 8 + 16 + 1008 * (2 if precision == "bf16" else 4))
+        kernels = {
+            "aev_backward": {"ms_per_launch": kt["aev_backward"], "bound": "hbm",
+                             "algorithmic_bytes_per_launch": bwd_bytes,
+                             "achieved": bwd_bytes / (kt["aev_backward"] * 1e-3) / 1e9, "unit": "GB/s",
+                             "peak": hbm},
+            "aev_forward": {"ms_per_launch": kt["aev_forward"], "bound": "hbm",
+                            "algorithmic_bytes_per_launch": fwd_bytes,
+                            "achieved": fwd_bytes / (kt["aev_forward"] * 1e-3) / 1e9, "unit": "GB/s",
+                            "peak": hbm},
+            "mlp": {"ms_per_launch": mlp_ms, "bound": "tensor", "algorithmic_flop_per_launch": flops,
+                    "achieved": mlp_tf, "unit": "TFLOP/s", "peak": tf_burst},
+        }
+        for k in kernels.values():
+            k["frac"] = k["achieved"] / k["peak"]
+        res["kernels"] = kernels
+        res["kernels"]["mean_radial_neighbors"] = mean_nbr
+        top = max(("aev_backward", "aev_forward", "mlp"), key=lambda k: kernels[k]["ms_per_launch"])
+        kd = kernels[top]
+        names = {"aev_backward": "k_aev_backward", "aev_forward": "k_aev_forward", "mlp": "k_mlp_fused"}
+        traffic = profile_traffic(names[top], args.workload)
+        res["roofline"] = {"bound": kd["bound"], "kernel": names[top], "achieved": kd["achieved"],
+                           "peak": kd["peak"], "unit": kd["unit"], "frac": kd["frac"],
+                           "traffic": traffic,
+                           "peak_source": f"{src} {'HBM copy' if kd['bound'] == 'hbm' else 'bf16 burst'}",
+                           "ms_per_launch": kd["ms_per_launch"],
+                           "algorithmic_per_launch": kd.get("algorithmic_bytes_per_launch",
+                                                            kd.get("algorithmic_flop_per_launch"))}
         if precision != "fp32":
             _, pot32, eng32 = make_engine(args.workload, "fp32", device, seed=rank)
             ms32 = time_steps(eng32, max(5, args.steps // 3), 3, flush)
@@ -433,6 +570,8 @@ def main():
             res["ensemble_98k"] = ensemble_98k(device, 5, 3, flush)
         if not args.skip_serving:
             res["serving"] = serving_run(device)
+        if args.nve_drift_steps > 0:
+            res["nve_drift"] = nve_drift(device, args.nve_drift_steps)
         if not args.no_cpu_baseline:
             res["cpu_baseline"] = cpu_baseline(box, w["n_models"])
         print(json.dumps(res), flush=True)

@@ -58,7 +58,7 @@ class MDEngine:
         coordinates = np.asarray(coordinates, dtype=np.float64)
         natoms = [species.shape[0]] if natoms is None else list(natoms)
         cells = None if cell is None else np.asarray(cell).reshape(-1, 3, 3)
-        self.layout = pot.layout(species, natoms, cells)
+        self.layout = pot.layout(species, natoms, cells, reach=pot.aev_cfg.radial_cutoff + float(skin))
         self.n = self.layout.n
         self.dt = dt_fs / 1000.0
         self.skin = float(skin)

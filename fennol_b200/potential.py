@@ -127,6 +127,16 @@ def aev_params(cfg: AEVConfig) -> _lib.AEVParams:
     return p
 
 
+def min_image_ok(cell, reach: float) -> bool:
+    """Minimum image finds every pair within ``reach`` when each perpendicular
+    width of the cell is at least ``2 * reach``."""
+    if cell is None:
+        return True
+    recip = np.linalg.inv(np.asarray(cell, np.float64).reshape(3, 3))
+    widths = 1.0 / np.linalg.norm(recip, axis=0)
+    return bool(np.all(widths >= 2.0 * reach))
+
+
 @dataclasses.dataclass
 class Capacities:
     """Row lengths of the neighbour lists (reference state keys ``npairs``,
@@ -317,6 +327,8 @@ class ANIPotential:
     ``"bf16x3"`` (tcgen05 tensor-core GEMMs with 1, 2 or 3 BF16 products).
     ``bf16_weights`` rounds the kernels to BFloat16 (a model stored in BF16);
     bf16x2 is exact in the weights for such a model.
+    ``minimum_image``: True / False force the minimum-image or the general
+    periodic search; None (default) picks per system (see :meth:`layout`).
     Energies are returned in Hartree (FeNNol's default model unit) and
     forces in Hartree/Angstrom, unless ``energy_unit="kcalpermol"``.
     """
@@ -324,7 +336,7 @@ class ANIPotential:
     def __init__(self, aev: AEVConfig = AEVConfig(), mlp: MLPConfig = MLPConfig(),
                  weights: Optional[Weights] = None, precision: str = "fp32", device="cuda",
                  seed: int = 0, n_models: int = 1, energy_unit: str = "Ha",
-                 minimum_image: bool = True, output_scale: float = 1.0,
+                 minimum_image: Optional[bool] = None, output_scale: float = 1.0,
                  bf16_weights: bool = False):
         if precision not in _lib.PRECISIONS:
             raise ValueError(f"precision must be one of {list(_lib.PRECISIONS)}")
@@ -353,9 +365,24 @@ class ANIPotential:
         self._tc_launches = 6
 
     # ------------------------------------------------------------------ layout
-    def layout(self, species, natoms, cells=None) -> BatchLayout:
+    def layout(self, species, natoms, cells=None, reach: Optional[float] = None) -> BatchLayout:
+        """Batch layout.  With ``minimum_image=None`` each periodic system uses
+        the minimum-image search when its cell is at least twice ``reach``
+        (default: the radial cutoff) wide in every direction, and the general
+        periodic search over cell images otherwise."""
         sidx = self.aev_cfg.species_index(np.asarray(species))
-        return BatchLayout(sidx, natoms, cells, self.minimum_image, self.device)
+        mi = self.minimum_image
+        if mi is None:
+            r = self.aev_cfg.radial_cutoff if reach is None else reach
+            nsys = len(np.asarray(natoms).reshape(-1))
+            if cells is None:
+                mi = True
+            else:
+                cl = cells if isinstance(cells, (list, tuple)) else list(np.asarray(cells).reshape(-1, 3, 3))
+                if len(cl) == 1 and nsys > 1:
+                    cl = cl * nsys
+                mi = [min_image_ok(c, r) for c in cl]
+        return BatchLayout(sidx, natoms, cells, mi, self.device)
 
     def buffers(self, layout: BatchLayout, skin: float = 0.0, cap: Optional[int] = None,
                 cap_radial: Optional[int] = None):
@@ -475,8 +502,8 @@ class ANIPotential:
         species = np.asarray(species)
         if natoms is None:
             natoms = [species.shape[0]]
-        layout = self.layout(species, natoms, cells)
         rc = self.aev_cfg.radial_cutoff if cutoff is None else cutoff
+        layout = self.layout(species, natoms, cells, reach=rc)
         cap = layout.estimate_capacity(rc)
         coords = torch.as_tensor(np.asarray(coordinates), dtype=torch.float32).to(self.device).contiguous()
         status = torch.zeros(_lib.STATUS_WORDS, dtype=torch.int32, device=self.device)

@@ -46,7 +46,7 @@ from ._lib import call
 from .md import KB_KCALMOL, MASS_DA_TO_MD
 from .params import ATOMIC_MASSES
 from .potential import (MAX_ROW, ANIPotential, BatchLayout, GraphBuffers, HARTREE_TO_KCALMOL,
-                        Workspace, _ptr)
+                        Workspace, _ptr, min_image_ok)
 
 
 @dataclasses.dataclass
@@ -88,13 +88,7 @@ class ServeResult:
 
 
 def _min_image_ok(cell: Optional[np.ndarray], reach: float) -> bool:
-    """Minimum image is exact when every perpendicular width of the cell is
-    at least twice the search radius; smaller cells use periodic images."""
-    if cell is None:
-        return True
-    recip = np.linalg.inv(np.asarray(cell, np.float64))
-    widths = 1.0 / np.linalg.norm(recip, axis=0)
-    return bool(np.all(widths >= 2.0 * reach))
+    return min_image_ok(cell, reach)
 
 
 def _pinned(shape, dtype) -> torch.Tensor:

@@ -23,11 +23,11 @@ def pot(cuda_device):
 
 
 def _gpu_pairs(pot, xyz, sp, nat, cells, cutoff, minimum_image=True):
-    pot.minimum_image = minimum_image
+    prev, pot.minimum_image = pot.minimum_image, minimum_image
     try:
         nj, ns, nn, _ = pot.neighbor_lists(xyz, sp, nat, cells, cutoff)
     finally:
-        pot.minimum_image = True
+        pot.minimum_image = prev
     canon, sym = graph_fp32.canonical_from_ell(nj, unpack_shifts(ns), nn)
     return canon, sym, nj, ns, nn
 
