@@ -339,7 +339,7 @@ def ensemble_98k(device, steps, warmup, flush):
     return out
 
 
-DRIFT_OUTPUT_SCALE = 0.005
+DRIFT_OUTPUT_SCALE = 0.002
 
 
 def nve_drift(device, steps, workload="water98k", every=100):
