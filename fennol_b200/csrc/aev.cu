@@ -26,7 +26,6 @@ constexpr int kAevWarps = 8;
 constexpr int kMaxS = 8;
 constexpr int kMaxP = kMaxS * (kMaxS + 1) / 2;
 constexpr int kCapA = FENNOL_MAX_ANGULAR_NEIGHBORS;
-constexpr float kPi = 3.14159265358979323846f;
 
 struct AevConst {
   int S, P, RD, AD, AS, F;
@@ -127,6 +126,7 @@ struct Stage {
   float2* af;    // [kCapA] angular (fc, dfc)
   int* aslot;    // [kCapA] radial row position of each angular neighbour
   int* cntw;     // [32] per-species counters
+  int* rslot;    // [cap] radial row position of each sorted radial entry (tangent kernel only)
 };
 
 __host__ __device__ __forceinline__ size_t stage_bytes(int cap) {
@@ -143,6 +143,7 @@ __device__ __forceinline__ Stage carve_stage(char* base, int cap) {
   st.tkey = (int*)((char*)st.af + (size_t)kCapA * 8);
   st.aslot = st.tkey + cap;
   st.cntw = st.aslot + kCapA;
+  st.rslot = nullptr;
   return st;
 }
 
@@ -173,7 +174,7 @@ __device__ __forceinline__ float zeta_pow(float x, int n, float f) {
 // Warp-collective: stage row i.  Returns, in lanes s < S, the per-species
 // radial and angular counts and exclusive offsets.  Lanes holding the same
 // species are grouped with __match_any_sync; per-warp counters live in `cntw`.
-template <bool kGrad>
+template <bool kGrad, bool kRslot = false>
 __device__ __forceinline__ void stage_row(const Stage& st, int* cntw, const float4* __restrict__ xyzs, float4 pi,
                                           const float* c, const int* __restrict__ nbr_j,
                                           const unsigned* __restrict__ nbr_shift, size_t row, int cnt,
@@ -251,6 +252,7 @@ __device__ __forceinline__ void stage_row(const Stage& st, int* cntw, const floa
       float d = sqrtf(fmaxf(v.w, 1e-5f));
       float fc = d < K.rc ? 0.5f * cosf(d * K.pi_rc) + 0.5f : 0.f;
       st.rd[pos_r] = make_float2(d, 0.25f * fc);
+      if (kRslot) st.rslot[pos_r] = k;
       if (pos_a >= 0 && pos_a < kCapA) {
         float inv = 1.0f / fmaxf(d, 1e-5f);
         st.au[pos_a] = make_float4(v.x * inv, v.y * inv, v.z * inv, d);
@@ -605,6 +607,152 @@ k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ a
   if (lane == 0) atomicAdd(forces + i, make_float4(fx, fy, fz, 0.f));
 }
 
+// --------------------------------------------------------------------------------
+// Tangent (forward mode): t = dAEV/dx . u for a displacement field u.  With
+// F = -dE/dx, the force term of a training loss differentiates
+// sum_i <dE/dAEV_i, t_i> with respect to the network parameters, which needs
+// the AEV tangent along u = dL/dF (the second-order term of jax.grad over a
+// force loss, training/utils.py:140-525).
+// --------------------------------------------------------------------------------
+__host__ __device__ __forceinline__ size_t jvp_bytes(int cap) {
+  return (stage_bytes(cap) + (size_t)cap * (4 + 16 + 8) + 15) / 16 * 16;
+}
+
+template <int RD, int AD, int AS>
+__global__ void __launch_bounds__(kAevWarps * 32)
+k_aev_tangent(const float4* __restrict__ xyzs, int n, const int* __restrict__ atom_sys,
+              const float* __restrict__ sys_cell, const int* __restrict__ nbr_j,
+              const unsigned* __restrict__ nbr_shift, const int* __restrict__ nbr_count, int cap,
+              const AevConst K, const int* __restrict__ atom_row, const float4* __restrict__ du,
+              float* __restrict__ out, int ld, int* status) {
+  extern __shared__ __align__(16) char smem_c[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i = blockIdx.x * kAevWarps + warp;
+  if (i >= n) return;
+  const int S = K.S;
+  char* base = smem_c + (size_t)warp * jvp_bytes(cap);
+  Stage st = carve_stage(base, cap);
+  float4* tanw = (float4*)(base + stage_bytes(cap));  // [cap] (u_j - u_i) / d, d-dot (row order)
+  float2* tanr = (float2*)(tanw + cap);                // [cap] d-dot, 0.25 fc'(d)  (row order)
+  st.rslot = (int*)(tanr + cap);                       // [cap]
+  const float4 pi = xyzs[i];
+  const float4 ui = du[i];
+  float c[9];
+  load_cell(sys_cell, atom_sys[i], c);
+  int cnt = nbr_count[i];
+  if (cnt > cap) cnt = cap;
+  const size_t row = (size_t)i * cap;
+  int cnt_r, off_r, cnt_a, off_a, na;
+  stage_row<true, true>(st, st.cntw, xyzs, pi, c, nbr_j, nbr_shift, row, cnt, K, lane, cnt_r, off_r, cnt_a,
+                        off_a, na);
+  if (na > kCapA && lane == 0) status_set(status, ST_ANG_OVERFLOW);
+
+  // per-neighbour tangents: d-dot = r.(u_j - u_i)/d and (u_j - u_i)/d
+  for (int k = lane; k < cnt; k += 32) {
+    const float4 v = st.tmp[k];
+    const float4 uj = du[__ldg(nbr_j + row + k)];
+    const float rx = uj.x - ui.x, ry = uj.y - ui.y, rz = uj.z - ui.z;
+    const float d = sqrtf(fmaxf(v.w, 1e-5f));
+    const float inv = v.w > 1e-5f ? 1.0f / d : 0.f;  // safe_sqrt clip: no tangent below it
+    const float dd = (v.x * rx + v.y * ry + v.z * rz) * inv;
+    tanw[k] = make_float4(rx * inv, ry * inv, rz * inv, dd);
+    const float dfc = d < K.rc ? -0.5f * K.pi_rc * sinf(d * K.pi_rc) : 0.f;
+    tanr[k] = make_float2(dd, 0.25f * dfc);
+  }
+  __syncwarp();
+  const size_t orow = (size_t)atom_row[i] * ld;
+
+  // ---- radial: d/dt [0.25 fc(d) exp(-eta (d - R)^2)]
+  constexpr int nh = 32 / RD;
+  const int r_lane = lane % RD, h_lane = lane / RD;
+  const float sr = K.shift_r[r_lane], eta_r = K.eta_r;
+  for (int s = 0; s < S; ++s) {
+    const int ns = __shfl_sync(0xffffffffu, cnt_r, s);
+    const int os = __shfl_sync(0xffffffffu, off_r, s);
+    float acc = 0.f;
+    for (int t = h_lane; t < ns; t += nh) {
+      const float2 e = st.rd[os + t];
+      const float2 tr = tanr[st.rslot[os + t]];
+      const float x = e.x - sr;
+      acc = fmaf(fexp(-eta_r * x * x) * (tr.y - 2.f * eta_r * x * e.y), tr.x, acc);
+    }
+    if (nh == 2) acc += __shfl_xor_sync(0xffffffffu, acc, 16);
+    if (h_lane == 0) out[orow + s * RD + r_lane] = acc;
+  }
+
+  // ---- angular
+  const int FR = S * RD;
+  for (int col = lane; col < K.P * 32; col += 32) out[orow + FR + col] = 0.f;
+  const float c_ang = K.c_ang, eta_a = K.eta_a, zeta = K.zeta;
+  const unsigned present = __ballot_sync(0xffffffffu, lane < S && cnt_a > 0);
+  for (unsigned m1 = present; m1; m1 &= m1 - 1) {
+    const int s1 = __ffs(m1) - 1;
+    const int n1 = min(__shfl_sync(0xffffffffu, cnt_a, s1), kCapA);
+    const int o1 = __shfl_sync(0xffffffffu, off_a, s1);
+    for (unsigned m2 = m1; m2; m2 &= m2 - 1) {
+      const int s2 = __ffs(m2) - 1;
+      const int n2 = min(__shfl_sync(0xffffffffu, cnt_a, s2), kCapA);
+      const int o2 = __shfl_sync(0xffffffffu, off_a, s2);
+      int T = s1 == s2 ? n1 * (n1 - 1) / 2 : n1 * n2;
+      if (o1 + n1 > kCapA || o2 + n2 > kCapA) T = 0;
+      if (T == 0) continue;
+      const int p = triu_pair(s1, s2, S);
+      float acc[32];
+#pragma unroll
+      for (int k = 0; k < 32; ++k) acc[k] = 0.f;
+      for (int t0 = 0; t0 < T; t0 += 32) {
+        const int t = t0 + lane;
+        if (t < T) {
+          int a, b;
+          if (s1 == s2) {
+            tri_ab(t, a, b);
+            a += o1;
+            b += o1;
+          } else {
+            a = o1 + t / n2;
+            b = o2 + t % n2;
+          }
+          const float4 ua = st.au[a], ub = st.au[b];
+          const float2 fa = st.af[a], fb = st.af[b];
+          const float4 wa = tanw[st.aslot[a]], wb = tanw[st.aslot[b]];
+          const float cosang = ua.x * ub.x + ua.y * ub.y + ua.z * ub.z;
+          // d/dt of u_a . u_b with u = r / |r|
+          const float dcos = (wa.x * ub.x + wa.y * ub.y + wa.z * ub.z) - cosang * wa.w / ua.w +
+                             (wb.x * ua.x + wb.y * ua.y + wb.z * ua.z) - cosang * wb.w / ub.w;
+          const float ct = 0.95f * cosang, dct = 0.95f * dcos;
+          const float stt = sqrtf(fmaxf(1.0f - ct * ct, 1e-12f));
+          const float dstt = -ct * dct / stt;
+          const float f = c_ang * fa.x * fb.x;
+          const float df = c_ang * (fa.y * wa.w * fb.x + fa.x * fb.y * wb.w);
+          float A[AS], dA[AS];
+#pragma unroll
+          for (int z = 0; z < AS; ++z) {
+            const float cz = ct * K.cosz[z] + stt * K.sinz[z];
+            const float dcz = dct * K.cosz[z] + dstt * K.sinz[z];
+            const float bs = fmaxf(1.0f + cz, 0.f);
+            const float pw1 = zeta_pow(bs, K.zeta1_n, K.zeta1_f);  // (1 + cz)^(zeta - 1)
+            A[z] = f * pw1 * bs;
+            dA[z] = df * pw1 * bs + f * zeta * pw1 * dcz;
+          }
+          const float dm = 0.5f * (ua.w + ub.w), ddm = 0.5f * (wa.w + wb.w);
+#pragma unroll
+          for (int r = 0; r < AD; ++r) {
+            const float x = dm - K.shift_a[r];
+            const float B = fexp(-eta_a * x * x);
+            const float dB = -2.f * eta_a * x * ddm * B;
+#pragma unroll
+            for (int z = 0; z < AS; ++z) acc[r * AS + z] = fmaf(dA[z], B, fmaf(A[z], dB, acc[r * AS + z]));
+          }
+        }
+      }
+      const float v = transpose_reduce32(acc, lane);
+      __syncwarp();
+      out[orow + FR + p * 32 + lane] = v;
+    }
+  }
+}
+
+
 __global__ void k_pack(const float* __restrict__ coords, const int* __restrict__ sp, int n,
                        float4* __restrict__ xyzs) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -616,6 +764,7 @@ template <int RD, int AD, int AS>
 struct AevKernels {
   static constexpr auto fwd = k_aev_forward<RD, AD, AS>;
   static constexpr auto bwd = k_aev_backward<RD, AD, AS>;
+  static constexpr auto tan = k_aev_tangent<RD, AD, AS>;
 };
 
 // (RD, AD, AS) combinations compiled: radial 16/32 x angular (8,4) / (4,8).
@@ -713,6 +862,33 @@ extern "C" int fennol_aev_backward(const float* xyzs, int natoms, const int* ato
     ks.bwd<<<blocks, kAevWarps * 32, smem, (cudaStream_t)stream>>>(
         (const float4*)xyzs, natoms, atom_sys, sys_cell, nbr_j, nbr_shift, nbr_count, capacity, K,
         atom_row, daev, ld, (float4*)forces4, status);
+    return true;
+  });
+  if (!launched) return FENNOL_ERR_UNSUPPORTED;
+  FNL_CHECK_LAUNCH();
+  return FENNOL_OK;
+}
+
+extern "C" int fennol_aev_tangent(const float* xyzs, int natoms, const int* atom_sys,
+                                  const float* sys_cell, const int* nbr_j, const unsigned* nbr_shift,
+                                  const int* nbr_count, int capacity, const fennol_aev_params* p,
+                                  const int* atom_row, const float* du4, float* out, int ld, int* status,
+                                  void* stream) {
+  AevConst K;
+  if (!make_const(p, &K)) return FENNOL_ERR_UNSUPPORTED;
+  if (natoms < 0 || capacity <= 0 || ld < K.F) return FENNOL_ERR_INVALID;
+  if (natoms == 0) return FENNOL_OK;
+  if (!xyzs || !atom_sys || !nbr_j || !nbr_shift || !nbr_count || !atom_row || !du4 || !out)
+    return FENNOL_ERR_INVALID;
+  size_t bytes = (size_t)kAevWarps * jvp_bytes(capacity);
+  if (bytes > 200 * 1024) return FENNOL_ERR_UNSUPPORTED;
+  int blocks = (natoms + kAevWarps - 1) / kAevWarps;
+  bool launched = dispatch(K, [&](auto ks) {
+    size_t smem = set_smem((const void*)ks.tan, bytes);
+    if (!smem) return false;
+    ks.tan<<<blocks, kAevWarps * 32, smem, (cudaStream_t)stream>>>(
+        (const float4*)xyzs, natoms, atom_sys, sys_cell, nbr_j, nbr_shift, nbr_count, capacity, K,
+        atom_row, (const float4*)du4, out, ld, status);
     return true;
   });
   if (!launched) return FENNOL_ERR_UNSUPPORTED;

@@ -211,6 +211,20 @@ int fennol_aev_backward(const float* xyzs, int natoms, const int* atom_sys,
                         const int* atom_row, const float* daev, int ld, float* forces4,
                         int* status, void* stream);
 
+/*
+ * Forward-mode tangent of the AEV: out[atom_row[i]*ld + f] = sum_k
+ * dAEV_i,f/dx_k . du_k for a displacement field du4 (float32 [natoms*4],
+ * x, y, z, unused).  No counterpart call in the reference: jax.grad over a
+ * loss that contains forces (training/utils.py:140-525) forms this product
+ * inside XLA's second-order transpose; the training gradient uses it to
+ * differentiate sum_i <dE/dAEV_i, t_i> with respect to the network
+ * parameters.  float32 output, same row layout as fennol_aev_forward.
+ */
+int fennol_aev_tangent(const float* xyzs, int natoms, const int* atom_sys, const float* sys_cell,
+                       const int* nbr_j, const unsigned* nbr_shift, const int* nbr_count,
+                       int capacity, const fennol_aev_params* p, const int* atom_row,
+                       const float* du4, float* out, int ld, int* status, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Species-indexed MLP                                                       */
 /* ------------------------------------------------------------------------ */

@@ -193,3 +193,55 @@ def energy_and_forces(coordinates, species, natoms, weights: List[Dict], aev_cfg
     if return_aev:
         res["aev"] = emb.detach().numpy()
     return res
+
+
+def loss_and_grads(coordinates, species, natoms, model: Dict, aev_cfg, mlp_cfg, e_ref, f_ref,
+                   w_e: float = 1.0, w_f: float = 10.0, cells=None, minimum_image=True,
+                   dtype=torch.float64, graph: Optional[Graph] = None):
+    """Energy + force loss of one model and its gradient with respect to every
+    kernel and bias, by second-order autograd (what ``jax.value_and_grad``
+    over the loss of ``training/utils.py:140-525`` computes).
+
+    ``L = w_e * mean_b (E_b - e_ref_b)^2 + w_f * mean (F - f_ref)^2``.
+    Returns (loss, {symbol: [(dW, db), ...]}) as float64 numpy."""
+    coordinates = np.asarray(coordinates, dtype=np.float64)
+    natoms = np.asarray(natoms).reshape(-1)
+    if graph is None:
+        graph = Graph(coordinates, natoms, cells, None, aev_cfg.radial_cutoff, aev_cfg.angular_cutoff,
+                      minimum_image)
+    sidx = aev_cfg.species_index(species)
+    params = {sym: [(torch.tensor(np.asarray(w), dtype=dtype, requires_grad=True),
+                     torch.tensor(np.asarray(b), dtype=dtype, requires_grad=True)) for w, b in layers]
+              for sym, layers in model.items()}
+    x = torch.tensor(coordinates, dtype=dtype, requires_grad=True)
+    emb = aev(x, sidx, graph, aev_cfg)
+    eat = species_net(emb, sidx, params, aev_cfg.species_order, mlp_cfg.celu_alpha)
+    bidx = torch.as_tensor(graph.batch_index)
+    etot = torch.zeros(natoms.shape[0], dtype=dtype).index_add(0, bidx, eat)
+    (g,) = torch.autograd.grad(etot.sum(), x, create_graph=True)
+    forces = -g
+    e_ref = torch.as_tensor(np.asarray(e_ref, np.float64), dtype=dtype)
+    f_ref = torch.as_tensor(np.asarray(f_ref, np.float64), dtype=dtype).reshape(forces.shape)
+    loss = w_e * ((etot - e_ref) ** 2).mean() + w_f * ((forces - f_ref) ** 2).mean()
+    flat = [p for sym in aev_cfg.species_order for wb in params[sym] for p in wb]
+    gl = torch.autograd.grad(loss, flat, allow_unused=True)
+    out, k = {}, 0
+    for sym in aev_cfg.species_order:
+        layers = []
+        for w, b in params[sym]:
+            gw = gl[k] if gl[k] is not None else torch.zeros_like(w)
+            gb = gl[k + 1] if gl[k + 1] is not None else torch.zeros_like(b)
+            layers.append((gw.detach().numpy(), gb.detach().numpy()))
+            k += 2
+        out[sym] = layers
+    return float(loss.detach()), out
+
+
+def loss_value(coordinates, species, natoms, model: Dict, aev_cfg, mlp_cfg, e_ref, f_ref,
+               w_e: float = 1.0, w_f: float = 10.0, cells=None, graph: Optional[Graph] = None):
+    """The loss of :func:`loss_and_grads` alone (float64), for finite differences."""
+    r = energy_and_forces(coordinates, species, natoms, [model], aev_cfg, mlp_cfg, cells=cells,
+                          graph=graph)
+    e = np.asarray(r["energy"]) - np.asarray(e_ref, np.float64)
+    f = np.asarray(r["forces"]) - np.asarray(f_ref, np.float64).reshape(r["forces"].shape)
+    return float(w_e * np.mean(e ** 2) + w_f * np.mean(f ** 2))

@@ -149,3 +149,43 @@ def test_float32_oracle_close_to_float64(weights):
                                     cells=s.cell[None], dtype=torch.float32, graph=r64["graph"])
     assert abs(r32["energy"][0] - r64["energy"][0]) * 627.5 / s.natoms < 1e-4
     assert np.sqrt(((r32["forces"] - r64["forces"]) ** 2).mean()) * 627.5 < 0.05
+
+
+def test_loss_parameter_gradients_match_finite_differences():
+    """Second-order autograd of the energy + force loss (the training
+    gradient) against central differences, FP64, step 1e-4."""
+    from fennol_b200.params import AEVConfig, MLPConfig, init_weights
+    from fennol_b200.systems import molecule_batch
+    from oracle import ani_ref
+
+    cfg, mcfg = AEVConfig(), MLPConfig()
+    mols = molecule_batch(3, seed=31, nmin=8, nmax=14)
+    xyz = np.concatenate([m.coordinates for m in mols])
+    sp = np.concatenate([m.species for m in mols])
+    nat = [m.natoms for m in mols]
+    model = init_weights(cfg, mcfg, seed=3, bias_std=0.1)[0]
+    teacher = init_weights(cfg, mcfg, seed=4)
+    ref = ani_ref.energy_and_forces(xyz, sp, nat, teacher, cfg, mcfg)
+    graph = ani_ref.Graph(xyz, nat, None, None, cfg.radial_cutoff, cfg.angular_cutoff)
+    loss, grads = ani_ref.loss_and_grads(xyz, sp, nat, model, cfg, mcfg, ref["energy"], ref["forces"],
+                                         graph=graph)
+    assert abs(loss - ani_ref.loss_value(xyz, sp, nat, model, cfg, mcfg, ref["energy"], ref["forces"],
+                                         graph=graph)) < 1e-12 * max(1.0, loss)
+    rng = np.random.default_rng(0)
+    present = sorted({cfg.species_order[k] for k in cfg.species_index(sp)})
+    h = 1e-4
+    for _ in range(10):
+        sym = present[int(rng.integers(len(present)))]
+        layer = int(rng.integers(4))
+        which = int(rng.integers(2))
+        arr = model[sym][layer][which]
+        idx = tuple(int(rng.integers(n)) for n in arr.shape)
+        orig = arr[idx]
+        arr[idx] = orig + h
+        lp = ani_ref.loss_value(xyz, sp, nat, model, cfg, mcfg, ref["energy"], ref["forces"], graph=graph)
+        arr[idx] = orig - h
+        lm = ani_ref.loss_value(xyz, sp, nat, model, cfg, mcfg, ref["energy"], ref["forces"], graph=graph)
+        arr[idx] = orig
+        fd = (lp - lm) / (2 * h)
+        g = grads[sym][layer][which][idx]
+        assert abs(fd - g) <= 1e-5 * abs(g) + 1e-9 * max(1.0, loss), (sym, layer, which, idx, fd, g)
