@@ -129,17 +129,21 @@ struct Stage {
   int* rslot;    // [cap] radial row position of each sorted radial entry (tangent kernel only)
 };
 
-__host__ __device__ __forceinline__ size_t stage_bytes(int cap) {
+// `with_rd`: the sorted radial entries (d, 0.25 fc) are kept (forward and
+// tangent); the adjoint works from the unsorted rows and leaves them out.
+__host__ __device__ __forceinline__ size_t stage_bytes(int cap, bool with_rd = true) {
   // rounded to 16 bytes so that every per-warp carve-up keeps float4 alignment
-  return ((size_t)cap * (16 + 4 + 8) + (size_t)kCapA * (16 + 8 + 4) + 32 * 4 + 15) / 16 * 16;
+  return ((size_t)cap * (16 + 4 + (with_rd ? 8 : 0)) + (size_t)kCapA * (16 + 8 + 4) + 32 * 4 + 15) / 16 * 16;
 }
 
-__device__ __forceinline__ Stage carve_stage(char* base, int cap) {
+__device__ __forceinline__ Stage carve_stage(char* base, int cap, bool with_rd = true) {
   Stage st;
   st.tmp = (float4*)base;
   st.au = (float4*)(base + (size_t)cap * 16);
-  st.rd = (float2*)(base + (size_t)cap * 16 + (size_t)kCapA * 16);
-  st.af = (float2*)((char*)st.rd + (size_t)cap * 8);
+  char* next = base + (size_t)cap * 16 + (size_t)kCapA * 16;
+  st.rd = with_rd ? (float2*)next : nullptr;
+  if (with_rd) next += (size_t)cap * 8;
+  st.af = (float2*)next;
   st.tkey = (int*)((char*)st.af + (size_t)kCapA * 8);
   st.aslot = st.tkey + cap;
   st.cntw = st.aslot + kCapA;
@@ -174,7 +178,7 @@ __device__ __forceinline__ float zeta_pow(float x, int n, float f) {
 // Warp-collective: stage row i.  Returns, in lanes s < S, the per-species
 // radial and angular counts and exclusive offsets.  Lanes holding the same
 // species are grouped with __match_any_sync; per-warp counters live in `cntw`.
-template <bool kGrad, bool kRslot = false>
+template <bool kGrad, bool kRslot = false, bool kRd = true>
 __device__ __forceinline__ void stage_row(const Stage& st, int* cntw, const float4* __restrict__ xyzs, float4 pi,
                                           const float* c, const int* __restrict__ nbr_j,
                                           const unsigned* __restrict__ nbr_shift, size_t row, int cnt,
@@ -251,7 +255,7 @@ __device__ __forceinline__ void stage_row(const Stage& st, int* cntw, const floa
       float4 v = st.tmp[k];
       float d = sqrtf(fmaxf(v.w, 1e-5f));
       float fc = d < K.rc ? 0.5f * cosf(d * K.pi_rc) + 0.5f : 0.f;
-      st.rd[pos_r] = make_float2(d, 0.25f * fc);
+      if (kRd) st.rd[pos_r] = make_float2(d, 0.25f * fc);
       if (kRslot) st.rslot[pos_r] = k;
       if (pos_a >= 0 && pos_a < kCapA) {
         float inv = 1.0f / fmaxf(d, 1e-5f);
@@ -427,7 +431,7 @@ k_aev_forward(const float4* __restrict__ xyzs, int n, const int* __restrict__ at
 constexpr int kMaxBlk = kMaxP;  // species-pair blocks of one centre atom
 
 __host__ __device__ __forceinline__ size_t bwd_bytes(int S, int RD, int cap) {
-  return (stage_bytes(cap) + (size_t)cap * 12 + (size_t)S * (RD + 1) * 4 + (2 * kMaxBlk + 2) * 4 + 15) / 16 * 16;
+  return (stage_bytes(cap, false) + (size_t)S * (RD + 1) * 4 + (2 * kMaxBlk + 2) * 4 + 15) / 16 * 16;
 }
 
 template <int RD, int AD, int AS>
@@ -443,11 +447,11 @@ k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ a
   if (i >= n) return;
   const int S = K.S;
   char* base = smem_c + (size_t)warp * bwd_bytes(S, RD, cap);
-  Stage st = carve_stage(base, cap);
-  float* gxs = (float*)(base + stage_bytes(cap));                     // [cap] x, y, z gradients
-  float* gys = gxs + cap;
-  float* gzs = gys + cap;
-  float* gr = gzs + cap;                                              // [S][RD+1]
+  Stage st = carve_stage(base, cap, false);
+  // the edge vectors in st.tmp[k] are replaced by the gradient of the energy
+  // with respect to edge k (x, y, z) once the radial pass has read them
+  float* gk = reinterpret_cast<float*>(st.tmp);
+  float* gr = (float*)(base + stage_bytes(cap, false));               // [S][RD+1]
   int* blkw = (int*)(gr + S * (RD + 1));                              // block table
 
   const float* g = daev + (size_t)atom_row[i] * ld;
@@ -460,10 +464,11 @@ k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ a
   if (cnt > cap) cnt = cap;
   const size_t row = (size_t)i * cap;
   int cnt_r, off_r, cnt_a, off_a, na;
-  stage_row<true>(st, st.cntw, xyzs, pi, c, nbr_j, nbr_shift, row, cnt, K, lane, cnt_r, off_r, cnt_a, off_a, na);
+  stage_row<true, false, false>(st, st.cntw, xyzs, pi, c, nbr_j, nbr_shift, row, cnt, K, lane, cnt_r, off_r,
+                                cnt_a, off_a, na);
   if (na > kCapA && lane == 0) status_set(status, ST_ANG_OVERFLOW);
 
-  // ---- radial: lane per neighbour (row order), gradient into grad[k]
+  // ---- radial: lane per neighbour (row order), gradient into gk[4k..4k+2]
   for (int k = lane; k < cnt; k += 32) {
     const float4 v = st.tmp[k];
     const int sj = st.tkey[k] & 0xFF;
@@ -484,9 +489,7 @@ k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ a
       dEdd = fmaf(grow[r] * e, dfc - 2.f * K.eta_r * x * fc, dEdd);
     }
     float sc = v.w > 1e-5f ? 0.25f * dEdd / d : 0.f;
-    gxs[k] = sc * v.x;
-    gys[k] = sc * v.y;
-    gzs[k] = sc * v.z;
+    st.tmp[k] = make_float4(sc * v.x, sc * v.y, sc * v.z, 0.f);
   }
   __syncwarp();
 
@@ -579,19 +582,20 @@ k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ a
     const float dEdc = cfab * Th * (-0.95f / stt);
     const float ia = dEdc / ua.w, ib = dEdc / ub.w;
     const int sa_ = st.aslot[a], sb_ = st.aslot[b];
-    atomicAdd(gxs + sa_, dEdda * ua.x + ia * (ub.x - cosang * ua.x));
-    atomicAdd(gys + sa_, dEdda * ua.y + ia * (ub.y - cosang * ua.y));
-    atomicAdd(gzs + sa_, dEdda * ua.z + ia * (ub.z - cosang * ua.z));
-    atomicAdd(gxs + sb_, dEddb * ub.x + ib * (ua.x - cosang * ub.x));
-    atomicAdd(gys + sb_, dEddb * ub.y + ib * (ua.y - cosang * ub.y));
-    atomicAdd(gzs + sb_, dEddb * ub.z + ib * (ua.z - cosang * ub.z));
+    atomicAdd(gk + 4 * sa_, dEdda * ua.x + ia * (ub.x - cosang * ua.x));
+    atomicAdd(gk + 4 * sa_ + 1, dEdda * ua.y + ia * (ub.y - cosang * ua.y));
+    atomicAdd(gk + 4 * sa_ + 2, dEdda * ua.z + ia * (ub.z - cosang * ua.z));
+    atomicAdd(gk + 4 * sb_, dEddb * ub.x + ib * (ua.x - cosang * ub.x));
+    atomicAdd(gk + 4 * sb_ + 1, dEddb * ub.y + ib * (ua.y - cosang * ub.y));
+    atomicAdd(gk + 4 * sb_ + 2, dEddb * ub.z + ib * (ua.z - cosang * ub.z));
   }
   __syncwarp();
 
   // ---- scatter: F_j -= g, F_i += sum g
   float fx = 0.f, fy = 0.f, fz = 0.f;
   for (int k = lane; k < cnt; k += 32) {
-    const float gx = gxs[k], gy = gys[k], gz = gzs[k];
+    const float4 gv = st.tmp[k];
+    const float gx = gv.x, gy = gv.y, gz = gv.z;
     int j = __ldg(nbr_j + row + k);
     atomicAdd(forces + j, make_float4(-gx, -gy, -gz, 0.f));
     fx += gx;

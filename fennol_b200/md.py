@@ -29,7 +29,7 @@ import torch
 
 from . import _lib
 from ._lib import call
-from .params import ATOMIC_MASSES
+from .params import atomic_masses
 from .potential import ANIPotential, C_ptr, GraphBuffers, HARTREE_TO_KCALMOL, Workspace, _ptr
 
 # atomic-unit constants of src/fennol/utils/atomic_units.py
@@ -68,7 +68,7 @@ class MDEngine:
             nblist_stride = max(1, int(math.floor(self.skin / 2.0 * 40.0 / dt_fs))) if skin > 0 else 1
         self.nblist_stride = nblist_stride
         self.check_every = check_every
-        mass_da = np.array([ATOMIC_MASSES[int(z)] for z in species], dtype=np.float64)
+        mass_da = atomic_masses(species)
         mass = mass_da * MASS_DA_TO_MD
         self.mass = mass
         kT = KB_KCALMOL * temperature

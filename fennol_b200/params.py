@@ -30,6 +30,21 @@ ATOMIC_MASSES = {
     15: 30.973762, 16: 32.06, 17: 35.45,
 }
 
+
+
+def atomic_masses(species) -> np.ndarray:
+    """Masses (Da, float64) of an array of atomic numbers; unknown elements raise."""
+    z = np.asarray(species, dtype=np.int64)
+    table = _MASS_TABLE[np.clip(z, 0, _MASS_TABLE.shape[0] - 1)]
+    if z.size and (z.min() < 0 or z.max() >= _MASS_TABLE.shape[0] or np.any(table == 0)):
+        raise ValueError("atomic number without a mass in ATOMIC_MASSES")
+    return table
+
+
+_MASS_TABLE = np.zeros(max(ATOMIC_MASSES) + 1)
+for _z, _m in ATOMIC_MASSES.items():
+    _MASS_TABLE[_z] = _m
+
 ANI2X_SPECIES = ("H", "C", "N", "O", "S", "F", "Cl")
 
 # Last-layer scale of the random model used by MD workloads (see init_weights).

@@ -44,7 +44,7 @@ import torch
 from . import _lib
 from ._lib import call
 from .md import KB_KCALMOL, MASS_DA_TO_MD
-from .params import ATOMIC_MASSES
+from .params import atomic_masses
 from .potential import (MAX_ROW, ANIPotential, BatchLayout, GraphBuffers, HARTREE_TO_KCALMOL,
                         Workspace, _ptr, min_image_ok)
 
@@ -233,7 +233,7 @@ class _MDLane:
             vs.append(torch.tensor(self._velocities(r), device=dev))
             f4s.append(f4)
             steps.append(torch.zeros(1, dtype=torch.int64, device=dev))
-        masses = np.concatenate([[ATOMIC_MASSES[int(z)] for z in np.asarray(r.species)] for r in reqs])
+        masses = atomic_masses(b.species)
         mass = masses * MASS_DA_TO_MD
         x = torch.cat(xs).contiguous()
         st = dict(batch=b, x=x, v=torch.cat(vs).contiguous(),
@@ -260,29 +260,20 @@ class _MDLane:
     def _velocities(self, r: ServeRequest) -> np.ndarray:
         if r.velocities is not None:
             return np.asarray(r.velocities, np.float64)
-        mass = np.array([ATOMIC_MASSES[int(z)] for z in np.asarray(r.species)]) * MASS_DA_TO_MD
+        mass = atomic_masses(r.species) * MASS_DA_TO_MD
         rng = np.random.default_rng(r.seed)
         return rng.standard_normal((r.natoms, 3)) * np.sqrt(self.e.kT / mass)[:, None]
 
     def _build(self, st):
-        """Full list build at the current positions (capacity regrown as needed)."""
-        pot, b = self.e.pot, st["batch"]
+        """Full list build at the current positions, enqueued without waiting:
+        a row overflow shows in the status words read at the end of the
+        segment, which then rolls back, regrows and runs again."""
+        b = st["batch"]
         s = self.stream.cuda_stream
-        for _ in range(6):
-            st["ws"].status.zero_()
-            st["g"].build(b.layout, st["coords"], st["ws"].status, s)
-            st["g"].filter(b.layout, st["coords"], st["ws"].status, s)
-            stat = st["ws"].status.cpu().numpy()
-            grow = None
-            if stat[_lib.ST_NBR_OVERFLOW] or stat[_lib.ST_FILTER_OVERFLOW]:
-                grow = pot.check_status(st["ws"], st["g"])
-            if grow is None:
-                break
-            st["g"] = GraphBuffers(b.layout, st["g"].cutoff, self.e.skin, *grow)
-            self.graphs.clear()
+        st["g"].build(b.layout, st["coords"], st["ws"].status, s)
+        st["g"].filter(b.layout, st["coords"], st["ws"].status, s)
         st["x_ref"].copy_(st["x"])
         st["flag"].zero_()
-        st["ws"].status.zero_()
         call("fennol_pack_atoms", st["coords"].data_ptr(), b.layout.t_species.data_ptr(), b.n,
              st["ws"].xyzs.data_ptr(), s)
 
@@ -311,6 +302,8 @@ class _MDLane:
         with torch.cuda.stream(self.stream):
             if admit and self.ready_event is not None:
                 self.stream.wait_event(self.ready_event)
+            if self.state is not None:
+                self.state["ws"].status.zero_()
             if changed:
                 if self.state is not None:
                     e.bytes_in_flight -= self.state["bytes"]
@@ -326,7 +319,6 @@ class _MDLane:
             st = self.state
             k = min(e.segment_steps, min(m["req"].md_steps - m["done"] for m in self.members))
             snap = (st["x"].clone(), st["v"].clone(), st["ws"].forces4.clone(), st["sys_step"].clone())
-            st["ws"].status.zero_()
             self._run(k, eager=changed)
             h_st = _pinned((_lib.STATUS_WORDS,), torch.int32)
             h_st.copy_(st["ws"].status, non_blocking=True)
@@ -373,8 +365,8 @@ class _MDLane:
                 st["coords"].copy_(st["x"].to(torch.float32))
                 st["g"] = GraphBuffers(st["batch"].layout, st["g"].cutoff, e.skin, *grow)
                 self.graphs.clear()
-                self._build(st)
                 st["ws"].status.zero_()
+                self._build(st)
                 self._run(fl["k"], eager=True)
                 fl["h_st"].copy_(st["ws"].status, non_blocking=True)
                 fl["ev"].record(self.stream)
