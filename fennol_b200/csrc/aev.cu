@@ -36,6 +36,7 @@ struct AevConst {
   float zeta_f;
   int zeta1_n;                      // the same split of zeta - 1
   float zeta1_f;
+  float dra, gc2a;                  // angular shift spacing, exp(-2 eta_a dra^2)
   float shift_r[32];
   float shift_a[32];
   float cosz[32], sinz[32];
@@ -73,6 +74,11 @@ bool make_const(const fennol_aev_params* p, AevConst* k) {
     k->zeta1_n = (int)z1;
     k->zeta1_f = (float)((double)p->zeta - 1.0 - z1);
     if (p->zeta < 1.0f || p->zeta > 64.0f) return false;
+  }
+  {
+    const double dra = (p->angular_cutoff - p->angular_start) / AD;
+    k->dra = (float)dra;
+    k->gc2a = (float)std::exp(-2.0 * (double)p->angular_eta * dra * dra);
   }
   for (int r = 0; r < 32; ++r) {
     k->shift_r[r] = r < RD ? (float)(p->radial_start + (p->radial_cutoff - p->radial_start) * r / RD) : 0.f;
@@ -158,6 +164,31 @@ __device__ __forceinline__ float exp2f_approx_pos(float x) {
   float y;
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
+}
+
+// Gaussians B[r] = exp(-eta (x0 - r dr)^2) of uniformly spaced shifts from
+// two exponentials: B[r+1] = B[r] g[r] with g[r] = exp(eta dr (2 (x0 - r dr) - dr))
+// and g[r+1] = g[r] c2, c2 = exp(-2 eta dr^2).  Every B[r] and g[r] stays below
+// its start value, so nothing overflows; when B[0] would be tiny (its
+// exponent below -80) the terms are evaluated one by one instead.
+template <int N>
+__device__ __forceinline__ void gauss_chain(float x0, float eta, float dr, float c2, float* B) {
+  if (eta * x0 * x0 > 80.f) {
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      const float x = x0 - (float)r * dr;
+      B[r] = fexp(-eta * x * x);
+    }
+    return;
+  }
+  float b = fexp(-eta * x0 * x0);
+  float g = fexp(eta * dr * (2.f * x0 - dr));
+#pragma unroll
+  for (int r = 0; r < N; ++r) {
+    B[r] = b;
+    b *= g;
+    g *= c2;
+  }
 }
 
 // x^zeta for x >= 0 as x^n * x^f with n = floor(zeta): the integer power by
@@ -407,11 +438,7 @@ k_aev_forward(const float4* __restrict__ xyzs, int n, const int* __restrict__ at
             A[z] = f * zeta_pow(1.0f + cz, K.zeta_n, K.zeta_f);
           }
           const float dm = 0.5f * (ua.w + ub.w);
-#pragma unroll
-          for (int r = 0; r < AD; ++r) {
-            float x = dm - K.shift_a[r];
-            B[r] = fexp(-eta_a * x * x);
-          }
+          gauss_chain<AD>(dm - K.shift_a[0], eta_a, K.dra, K.gc2a, B);
 #pragma unroll
           for (int r = 0; r < AD; ++r)
 #pragma unroll
@@ -559,10 +586,12 @@ k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ a
     }
     const float dm = 0.5f * (ua.w + ub.w);
     float Q = 0.f, Th = 0.f, Dm = 0.f;
+    float Bs[AD];
+    gauss_chain<AD>(dm - K.shift_a[0], eta_a, K.dra, K.gc2a, Bs);
 #pragma unroll
     for (int r = 0; r < AD; ++r) {
-      float x = dm - K.shift_a[r];
-      float Bv = fexp(-eta_a * x * x);
+      const float x = dm - K.shift_a[r];
+      const float Bv = Bs[r];
       float GA = 0.f, GAp = 0.f;
 #pragma unroll
       for (int z = 0; z < AS; ++z) {
@@ -579,8 +608,8 @@ k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ a
     const float dEddm = cfab * Dm;
     const float dEdda = 0.5f * dEddm + c_ang * fb * Q * fa2.y;
     const float dEddb = 0.5f * dEddm + c_ang * fa * Q * fb2.y;
-    const float dEdc = cfab * Th * (-0.95f / stt);
-    const float ia = dEdc / ua.w, ib = dEdc / ub.w;
+    const float dEdc = cfab * Th * (-0.95f * rsqrtf(fmaxf(1.0f - ct * ct, 1e-12f)));
+    const float ia = __fdividef(dEdc, ua.w), ib = __fdividef(dEdc, ub.w);
     const int sa_ = st.aslot[a], sb_ = st.aslot[b];
     atomicAdd(gk + 4 * sa_, dEdda * ua.x + ia * (ub.x - cosang * ua.x));
     atomicAdd(gk + 4 * sa_ + 1, dEdda * ua.y + ia * (ub.y - cosang * ua.y));
@@ -739,10 +768,12 @@ k_aev_tangent(const float4* __restrict__ xyzs, int n, const int* __restrict__ at
             dA[z] = df * pw1 * bs + f * zeta * pw1 * dcz;
           }
           const float dm = 0.5f * (ua.w + ub.w), ddm = 0.5f * (wa.w + wb.w);
+          float Bs[AD];
+          gauss_chain<AD>(dm - K.shift_a[0], eta_a, K.dra, K.gc2a, Bs);
 #pragma unroll
           for (int r = 0; r < AD; ++r) {
             const float x = dm - K.shift_a[r];
-            const float B = fexp(-eta_a * x * x);
+            const float B = Bs[r];
             const float dB = -2.f * eta_a * x * ddm * B;
 #pragma unroll
             for (int z = 0; z < AS; ++z) acc[r * AS + z] = fmaf(dA[z], B, fmaf(A[z], dB, acc[r * AS + z]));
