@@ -329,6 +329,8 @@ class ANIPotential:
     bf16x2 is exact in the weights for such a model.
     ``minimum_image``: True / False force the minimum-image or the general
     periodic search; None (default) picks per system (see :meth:`layout`).
+    ``use_graphs``: from the second call on the same batch (species, sizes,
+    cells) the whole evaluation is one CUDA-graph launch.
     Energies are returned in Hartree (FeNNol's default model unit) and
     forces in Hartree/Angstrom, unless ``energy_unit="kcalpermol"``.
     """
@@ -337,7 +339,7 @@ class ANIPotential:
                  weights: Optional[Weights] = None, precision: str = "fp32", device="cuda",
                  seed: int = 0, n_models: int = 1, energy_unit: str = "Ha",
                  minimum_image: Optional[bool] = None, output_scale: float = 1.0,
-                 bf16_weights: bool = False):
+                 bf16_weights: bool = False, use_graphs: bool = True):
         if precision not in _lib.PRECISIONS:
             raise ValueError(f"precision must be one of {list(_lib.PRECISIONS)}")
         _lib.load()
@@ -363,6 +365,10 @@ class ANIPotential:
         self.capacity_margin = 1.05
         self.add_neigh = 8
         self._tc_launches = 6
+        # repeated calls on the same batch replay one captured CUDA graph
+        self.use_graphs = use_graphs
+        self._graphs: Dict[tuple, dict] = {}
+        self._calls: Dict[tuple, int] = {}
 
     # ------------------------------------------------------------------ layout
     def layout(self, species, natoms, cells=None, reach: Optional[float] = None) -> BatchLayout:
@@ -451,6 +457,7 @@ class ANIPotential:
             layout = layout_fn()
             g, ws = self.buffers(layout)
             self._cache = {key: (layout, g, ws)}  # one cached layout
+            self._graphs, self._calls = {}, {}
         return self._cache[key]
 
     def energy_and_forces(self, coordinates, species, natoms=None, cells=None,
@@ -475,13 +482,20 @@ class ANIPotential:
             coords = coords.to(self.device, non_blocking=True)
         coords = coords.contiguous()
         stream = _stream(self.device)
+        gkey = (key, bool(want_forces))
+        rec = self._graphs.get(gkey) if self.use_graphs else None
+        if rec is not None and rec["g"] is g:
+            # same batch as the last calls: one graph launch for the whole evaluation
+            rec["coords"].copy_(coords, non_blocking=True)
+            rec["graph"].replay()
+            grow = self.check_status(ws, g)
+            if grow is None:
+                return ws.energy, (ws.forces if want_forces else None)
+            self._graphs.pop(gkey, None)
+            g = GraphBuffers(layout, g.cutoff, g.skin, grow[0], grow[1])
+            self._cache[key] = (layout, g, ws)
         for _attempt in range(4):
-            ws.status.zero_()
-            call("fennol_pack_atoms", coords.data_ptr(), layout.t_species.data_ptr(), layout.n,
-                 ws.xyzs.data_ptr(), stream)
-            g.build(layout, coords, ws.status, stream)
-            g.filter(layout, coords, ws.status, stream)
-            self.launch_forces(layout, g, ws, stream, want_forces)
+            self._launch_all(layout, g, ws, coords, stream, want_forces)
             grow = self.check_status(ws, g)
             if grow is None:
                 break
@@ -489,12 +503,35 @@ class ANIPotential:
             self._cache[key] = (layout, g, ws)
         else:
             raise RuntimeError("neighbour capacity did not converge")
-        forces = None
+        if self.use_graphs:
+            calls = self._calls.get(gkey, 0) + 1
+            self._calls = {gkey: calls}
+            if calls >= 2:  # a repeated batch: capture it once
+                self._capture(gkey, layout, g, ws, coords, want_forces)
+        return ws.energy, (ws.forces if want_forces else None)
+
+    def _launch_all(self, layout: BatchLayout, g: GraphBuffers, ws: Workspace, coords: torch.Tensor,
+                    stream: int, want_forces: bool):
+        """Every launch of one evaluation: pack, list build and filter, AEV,
+        MLP, energy sum, adjoint and force finalisation."""
+        ws.status.zero_()
+        call("fennol_pack_atoms", coords.data_ptr(), layout.t_species.data_ptr(), layout.n,
+             ws.xyzs.data_ptr(), stream)
+        g.build(layout, coords, ws.status, stream)
+        g.filter(layout, coords, ws.status, stream)
+        self.launch_forces(layout, g, ws, stream, want_forces)
         if want_forces:
             call("fennol_forces_finalize", ws.forces4.data_ptr(), layout.n, float(self.unit_scale),
                  ws.forces.data_ptr(), stream)
-            forces = ws.forces
-        return ws.energy, forces
+
+    def _capture(self, gkey, layout, g, ws, coords, want_forces):
+        buf = torch.empty_like(coords)
+        buf.copy_(coords)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            self._launch_all(layout, g, ws, buf, _stream(self.device), want_forces)
+        self._graphs = {gkey: {"graph": graph, "coords": buf, "g": g}}
+        # the replay recomputes the same values; results of this call stay valid
 
     def neighbor_lists(self, coordinates, species, natoms=None, cells=None, cutoff=None):
         """Per-atom rows (j, shift, count) of the pair list for ``cutoff``
