@@ -119,6 +119,7 @@ class _EFLane:
         self.e = engine
         self.stream = torch.cuda.Stream(engine.device)
         self.inflight = None
+        self.cap_hint = 0  # longest row seen so far (the reference's state["npairs"] role)
 
     def launch(self, reqs: List[ServeRequest]):
         e, pot = self.e, self.e.pot
@@ -127,7 +128,7 @@ class _EFLane:
             xyz = np.concatenate([np.asarray(r.coordinates, np.float32) for r in reqs]).astype(np.float32)
             h_x = torch.from_numpy(xyz).pin_memory()
             coords = h_x.to(e.device, non_blocking=True)
-            cap = b.layout.estimate_capacity(pot.aev_cfg.radial_cutoff)
+            cap = max(b.layout.estimate_capacity(pot.aev_cfg.radial_cutoff), self.cap_hint)
             g = GraphBuffers(b.layout, pot.aev_cfg.radial_cutoff, 0.0, cap, cap)
             ws = Workspace(pot, b.layout)
             st = self.stream.cuda_stream
@@ -167,6 +168,7 @@ class _EFLane:
             cap = (int(1.05 * st[_lib.ST_NBR_MAXCOUNT]) + 8 + 7) // 8 * 8
             if cap > MAX_ROW:
                 raise RuntimeError(f"neighbour rows longer than {MAX_ROW} are not supported")
+            self.cap_hint = max(self.cap_hint, cap)
             with torch.cuda.stream(self.stream):
                 g2 = GraphBuffers(b.layout, pot.aev_cfg.radial_cutoff, 0.0, cap, cap)
                 self._evaluate(b, fl["coords"], g2, ws, self.stream.cuda_stream)
@@ -210,15 +212,18 @@ class _MDLane:
         self.state = None
         self.inflight = None
         self.graphs: Dict[int, torch.cuda.CUDAGraph] = {}
+        self.cap_hint = (0, 0)  # longest skin / radial rows seen so far
         self.captures = 0
 
     # ---------------------------------------------------------------- state
-    def _new_state(self, keep: List[dict], new: List[tuple]):
+    def _new_state(self, keep: List[dict], new: List[tuple], b: Optional[_Batch] = None):
         """Device arrays of the next membership: continuing members' slices
-        of the current arrays followed by the new members."""
+        of the current arrays followed by the new members (``b``: the batch
+        layout of that membership when it was prepared ahead)."""
         e, pot, dev = self.e, self.e.pot, self.e.device
         reqs = [m["req"] for m in keep] + [r for r, _, _ in new]
-        b = _Batch(pot, reqs, pot.aev_cfg.radial_cutoff + e.skin, dev)
+        if b is None:
+            b = _Batch(pot, reqs, pot.aev_cfg.radial_cutoff + e.skin, dev)
         old = self.state
         xs, vs, f4s, steps = [], [], [], []
         for m in keep:
@@ -245,8 +250,8 @@ class _MDLane:
                   coords=x.to(torch.float32), x_ref=x.clone(),
                   flag=torch.zeros(1, dtype=torch.int32, device=dev))
         rc = pot.aev_cfg.radial_cutoff
-        cap = b.layout.estimate_capacity(rc + e.skin)
-        capr = b.layout.estimate_capacity(rc)
+        cap = max(b.layout.estimate_capacity(rc + e.skin), self.cap_hint[0])
+        capr = max(b.layout.estimate_capacity(rc), self.cap_hint[1])
         st["g"] = GraphBuffers(b.layout, rc, e.skin, cap, capr)
         st["ws"] = Workspace(pot, b.layout)
         st["ws"].forces4[:b.n].copy_(torch.cat(f4s))
@@ -292,7 +297,42 @@ class _MDLane:
         pot.launch_forces(lay, g, ws, s, True)
 
     # ------------------------------------------------------------ segments
-    def start_segment(self, admit: List[tuple]) -> bool:
+    def plan_next(self):
+        """While a segment runs on the device, lay out the next membership on
+        the host: the members that will still be running after it and the MD
+        requests ready now.  Requests that become ready later join one
+        segment after."""
+        e, fl = self.e, self.inflight
+        if fl is None:
+            return
+        k = fl["k"]
+        keep = [m for m in self.members if m["done"] + k < m["req"].md_steps]
+        admit = e._md_admits(sum(m["hi"] - m["lo"] for m in keep), pop=False)
+        self.prepared = None
+        if len(keep) == len(self.members) and not admit:
+            return  # unchanged membership: nothing to lay out
+        reqs = [m["req"] for m in keep] + [r for r, _, _ in admit]
+        if not reqs:
+            return
+        b = _Batch(e.pot, reqs, e.pot.aev_cfg.radial_cutoff + e.skin, e.device)
+        self.prepared = dict(keep=[m["req"] for m in keep], admit=list(admit), batch=b)
+
+    def take_prepared(self) -> Optional[tuple]:
+        """(admit, batch) of the prepared membership if it still applies, the
+        admitted requests removed from the ready list."""
+        p, self.prepared = getattr(self, "prepared", None), None
+        if p is None:
+            return None
+        keep = [m["req"] for m in self.members if m["done"] < m["req"].md_steps]
+        n = len(p["admit"])
+        if len(keep) != len(p["keep"]) or any(a is not b for a, b in zip(keep, p["keep"])):
+            return None
+        if len(self.ready) < n or any(a is not b for a, b in zip(self.ready[:n], p["admit"])):
+            return None
+        del self.ready[:n]
+        return p["admit"], p["batch"]
+
+    def start_segment(self, admit: List[tuple], batch: Optional[_Batch] = None) -> bool:
         """Retire finished members, admit new ones, enqueue the next segment.
         A segment right after a membership change is launched directly; later
         segments of the same membership replay a captured CUDA graph."""
@@ -311,7 +351,7 @@ class _MDLane:
                 if not keep and not admit:
                     self.members, self.state = [], None
                     return False
-                st, members = self._new_state(keep, admit)
+                st, members = self._new_state(keep, admit, batch)
                 st["bytes"] = e.bytes_per_atom_md * st["batch"].n
                 e.bytes_in_flight += st["bytes"]
                 self.state, self.members = st, members
@@ -364,6 +404,7 @@ class _MDLane:
                 st["sys_step"].copy_(steps)
                 st["coords"].copy_(st["x"].to(torch.float32))
                 st["g"] = GraphBuffers(st["batch"].layout, st["g"].cutoff, e.skin, *grow)
+                self.cap_hint = (max(self.cap_hint[0], grow[0]), max(self.cap_hint[1], grow[1]))
                 self.graphs.clear()
                 st["ws"].status.zero_()
                 self._build(st)
@@ -424,6 +465,26 @@ class ServingEngine:
         self.ef = _EFLane(self)
         self.md = _MDLane(self)
 
+    def _md_admits(self, running: int, pop: bool) -> List[tuple]:
+        """Ready MD requests, in order, that fit beside ``running`` atoms in
+        the MD lane's atom limit and in the HBM budget (the bytes of the
+        lane's current arrays are replaced by the next membership)."""
+        md = self.md
+        room = self.max_md_atoms - running
+        other = self.bytes_in_flight - (md.state["bytes"] if md.state else 0)
+        admit, atoms = [], running
+        for item in list(md.ready):
+            n_new = item[0].natoms
+            fits = n_new <= room and other + self.bytes_per_atom_md * (atoms + n_new) <= self.budget
+            if not fits and (admit or running or other):
+                break
+            admit.append(item)
+            room -= n_new
+            atoms += n_new
+        if pop:
+            del md.ready[:len(admit)]
+        return admit
+
     def _take(self, queue: Deque[ServeRequest], max_atoms: int, per_atom: int) -> List[ServeRequest]:
         out, atoms = [], 0
         while queue:
@@ -468,23 +529,15 @@ class ServingEngine:
                     self.ef.launch(batch)
                     progressed = True
             if self.md.inflight is None and (self.md.members or self.md.ready):
-                running = sum(m["hi"] - m["lo"] for m in self.md.members
-                              if m["done"] < m["req"].md_steps)
-                room = self.max_md_atoms - running
-                # bytes held by everything but the MD lane's current arrays,
-                # which the next membership replaces
-                other = self.bytes_in_flight - (self.md.state["bytes"] if self.md.state else 0)
-                admit, atoms = [], running
-                while self.md.ready:
-                    n_new = self.md.ready[0][0].natoms
-                    fits = n_new <= room and \
-                        other + self.bytes_per_atom_md * (atoms + n_new) <= self.budget
-                    if not fits and (admit or running or other):
-                        break
-                    admit.append(self.md.ready.pop(0))
-                    room -= n_new
-                    atoms += n_new
-                progressed |= self.md.start_segment(admit)
+                prepared = self.md.take_prepared()
+                if prepared is not None:
+                    progressed |= self.md.start_segment(*prepared)
+                else:
+                    running = sum(m["hi"] - m["lo"] for m in self.md.members
+                                  if m["done"] < m["req"].md_steps)
+                    progressed |= self.md.start_segment(self._md_admits(running, pop=True))
+                if self.md.inflight is not None:
+                    self.md.plan_next()
             if not progressed:
                 time.sleep(2e-5)
         torch.cuda.synchronize(self.device)
