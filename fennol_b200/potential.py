@@ -190,12 +190,14 @@ class BatchLayout:
         S = int(species_idx.max()) + 1 if n else 1
         row = np.zeros(n, np.int32)
         tiles_s, tiles_r = [], []
+        self.species_segments: List[Tuple[int, int, int]] = []  # (species, first row, atoms)
         off = 0
         for s in range(max(S, 1)):
             idx = np.nonzero(species_idx == s)[0]
             if idx.size == 0:
                 continue
             row[idx] = off + np.arange(idx.size)
+            self.species_segments.append((s, off, int(idx.size)))
             for t in range((idx.size + TILE - 1) // TILE):
                 tiles_s.append(s)
                 tiles_r.append(off + t * TILE)

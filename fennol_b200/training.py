@@ -114,8 +114,7 @@ class LossGradient:
         f_ref_t = torch.as_tensor(np.asarray(f_ref, np.float64), device=dev).reshape(N, 3)
         de = energy - e_ref_t
         df = forces.double() - f_ref_t
-        l_e = self.w_e * float((de ** 2).mean())
-        l_f = self.w_f * float((df ** 2).mean())
+        losses = torch.stack([(de ** 2).mean(), (df ** 2).mean()])
         c_sys = (2.0 * self.w_e / B) * de                      # dL/dE_b
         u = (2.0 * self.w_f / (3 * N)) * df                    # dL/dF
         du4 = torch.zeros((N, 4), dtype=torch.float32, device=dev)
@@ -126,26 +125,47 @@ class LossGradient:
         call("fennol_aev_tangent", ws.xyzs.data_ptr(), N, layout.t_atom_sys.data_ptr(), layout.t_cell.data_ptr(),
              g.rad_j.data_ptr(), g.rad_s.data_ptr(), g.rad_n.data_ptr(), g.cap_r, C_ptr(pot.params),
              layout.t_atom_row.data_ptr(), du4.data_ptr(), t.data_ptr(), d0, status.data_ptr(), _stream(dev))
-        if int(status[_lib.ST_ANG_OVERFLOW]):
-            raise RuntimeError(f"more than {_lib.MAX_ANGULAR_NEIGHBORS} angular neighbours around one atom")
         F = pot.aev_cfg.aev_length
         x = ws.x.float()
         if ws.x_lo is not None:
             x = x + ws.x_lo.float()
-        rows_of_atom = layout.t_atom_row.long()
-        c_atom = c_sys[layout.t_atom_sys.long()]
-        sidx = torch.as_tensor(layout.species_idx, device=dev)
+        # per-row energy seeds in the species-sorted row order of the AEV
+        c_row = torch.zeros(layout.rows, dtype=self.dtype, device=dev)
+        c_row[layout.t_atom_row.long()] = c_sys[layout.t_atom_sys.long()].to(self.dtype)
+        dev_grads: Dict[str, list] = {}
+        for k, row0, count in layout.species_segments:
+            sym = pot.aev_cfg.species_order[k]
+            sl = slice(row0, row0 + count)
+            dev_grads[sym] = network_loss_gradient(x[sl, :F].to(self.dtype), t[sl, :F].to(self.dtype),
+                                                   c_row[sl], self.layers[sym], pot.mlp_cfg.celu_alpha)
+        # one transfer for the whole gradient
+        parts, shapes = [], []
+        for sym in pot.aev_cfg.species_order:
+            for l, (W, b) in enumerate(self.layers[sym]):
+                if sym in dev_grads:
+                    gW, gb = dev_grads[sym][l]
+                else:
+                    gW, gb = torch.zeros_like(W), torch.zeros_like(b)
+                parts += [gW.reshape(-1), gb.reshape(-1)]
+                shapes += [tuple(W.shape), tuple(b.shape)]
+        flat = torch.cat([p_.double() for p_ in parts]).cpu().numpy()
         grads: Dict[str, List[Tuple[np.ndarray, np.ndarray]]] = {}
-        for k, sym in enumerate(pot.aev_cfg.species_order):
-            atoms = torch.nonzero(sidx == k).flatten()
-            layers = self.layers[sym]
-            if atoms.numel() == 0:
-                grads[sym] = [(np.zeros(tuple(W.shape)), np.zeros(tuple(b.shape))) for W, b in layers]
-                continue
-            rows = rows_of_atom[atoms]
-            gl = network_loss_gradient(x[rows, :F].to(self.dtype), t[rows, :F].to(self.dtype),
-                                       c_atom[atoms].to(self.dtype), layers, pot.mlp_cfg.celu_alpha)
-            grads[sym] = [(gW.double().cpu().numpy(), gb.double().cpu().numpy()) for gW, gb in gl]
+        pos, i = 0, 0
+        for sym in pot.aev_cfg.species_order:
+            layers = []
+            for _ in self.layers[sym]:
+                arrs = []
+                for _k in range(2):
+                    size = int(np.prod(shapes[i]))
+                    arrs.append(flat[pos:pos + size].reshape(shapes[i]))
+                    pos += size
+                    i += 1
+                layers.append(tuple(arrs))
+            grads[sym] = layers
+        l_e, l_f = (float(v) for v in (losses * torch.tensor([self.w_e, self.w_f], dtype=losses.dtype,
+                                                              device=dev)).cpu())
+        if int(status[_lib.ST_ANG_OVERFLOW]):
+            raise RuntimeError(f"more than {_lib.MAX_ANGULAR_NEIGHBORS} angular neighbours around one atom")
         terms = LossTerms(l_e + l_f, l_e, l_f, energy.cpu().numpy(), forces.cpu().numpy())
         return terms, grads
 
