@@ -85,6 +85,8 @@ _SIGNATURES = {
     "fennol_pack_atoms": (I, [P, P, I, P, P]),
     "fennol_aev_forward": (I, [P, I, P, P, P, P, P, I, C.POINTER(AEVParams), P, I, P, P, I, P, P]),
     "fennol_aev_backward": (I, [P, I, P, P, P, P, P, I, C.POINTER(AEVParams), P, P, I, P, P, P]),
+    "fennol_aev_backward_virial": (I, [P, I, P, P, P, P, P, I, C.POINTER(AEVParams), P, P, I, P, P, P, P]),
+    "fennol_virial_reduce": (I, [P, I, P, I, D, P, P]),
     "fennol_aev_tangent": (I, [P, I, P, P, P, P, P, I, C.POINTER(AEVParams), P, P, P, I, P, P]),
     "fennol_mlp_workspace_bytes": (SZ, [I, I, I, C.POINTER(MLPWeights)]),
     "fennol_mlp_energy_grad": (I, [I, I, I, P, P, C.POINTER(MLPWeights), P, P, P, P, P, SZ, P]),

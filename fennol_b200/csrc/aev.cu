@@ -461,13 +461,13 @@ __host__ __device__ __forceinline__ size_t bwd_bytes(int S, int RD, int cap) {
   return (stage_bytes(cap, false) + (size_t)S * (RD + 1) * 4 + (2 * kMaxBlk + 2) * 4 + 15) / 16 * 16;
 }
 
-template <int RD, int AD, int AS>
+template <int RD, int AD, int AS, bool kVir>
 __global__ void __launch_bounds__(kAevWarps * 32, 4)
 k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ atom_sys,
                const float* __restrict__ sys_cell, const int* __restrict__ nbr_j,
                const unsigned* __restrict__ nbr_shift, const int* __restrict__ nbr_count, int cap,
                const AevConst K, const int* __restrict__ atom_row, const float* __restrict__ daev,
-               int ld, float4* __restrict__ forces, int* status) {
+               int ld, float4* __restrict__ forces, float* __restrict__ atom_virial, int* status) {
   extern __shared__ __align__(16) char smem_c[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int i = blockIdx.x * kAevWarps + warp;
@@ -638,6 +638,38 @@ k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ a
     fz += __shfl_xor_sync(0xffffffffu, fz, o);
   }
   if (lane == 0) atomicAdd(forces + i, make_float4(fx, fy, fz, 0.f));
+
+  // ---- virial of this centre: sum over its edges of r (x) dE/dr
+  if (kVir) {
+    float v[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) v[q] = 0.f;
+    for (int k = lane; k < cnt; k += 32) {
+      const float4 gv = st.tmp[k];
+      float rx, ry, rz;
+      edge_vec(pi, xyzs[__ldg(nbr_j + row + k)], __ldg(nbr_shift + row + k), c, rx, ry, rz);
+      v[0] = fmaf(rx, gv.x, v[0]);
+      v[1] = fmaf(rx, gv.y, v[1]);
+      v[2] = fmaf(rx, gv.z, v[2]);
+      v[3] = fmaf(ry, gv.x, v[3]);
+      v[4] = fmaf(ry, gv.y, v[4]);
+      v[5] = fmaf(ry, gv.z, v[5]);
+      v[6] = fmaf(rz, gv.x, v[6]);
+      v[7] = fmaf(rz, gv.y, v[7]);
+      v[8] = fmaf(rz, gv.z, v[8]);
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+    }
+    if (lane < 9) {
+      float out = v[0];
+#pragma unroll
+      for (int q = 1; q < 9; ++q) out = lane == q ? v[q] : out;
+      atom_virial[(size_t)i * 9 + lane] = out;
+    }
+  }
 }
 
 // --------------------------------------------------------------------------------
@@ -798,7 +830,8 @@ __global__ void k_pack(const float* __restrict__ coords, const int* __restrict__
 template <int RD, int AD, int AS>
 struct AevKernels {
   static constexpr auto fwd = k_aev_forward<RD, AD, AS>;
-  static constexpr auto bwd = k_aev_backward<RD, AD, AS>;
+  static constexpr auto bwd = k_aev_backward<RD, AD, AS, false>;
+  static constexpr auto bwdv = k_aev_backward<RD, AD, AS, true>;
   static constexpr auto tan = k_aev_tangent<RD, AD, AS>;
 };
 
@@ -877,11 +910,10 @@ extern "C" int fennol_aev_forward(const float* xyzs, int natoms, const int* atom
   return FENNOL_OK;
 }
 
-extern "C" int fennol_aev_backward(const float* xyzs, int natoms, const int* atom_sys,
-                                   const float* sys_cell, const int* nbr_j, const unsigned* nbr_shift,
-                                   const int* nbr_count, int capacity, const fennol_aev_params* p,
-                                   const int* atom_row, const float* daev, int ld, float* forces4,
-                                   int* status, void* stream) {
+static int aev_backward_launch(const float* xyzs, int natoms, const int* atom_sys, const float* sys_cell,
+                               const int* nbr_j, const unsigned* nbr_shift, const int* nbr_count, int capacity,
+                               const fennol_aev_params* p, const int* atom_row, const float* daev, int ld,
+                               float* forces4, float* atom_virial, int* status, void* stream) {
   AevConst K;
   if (!make_const(p, &K)) return FENNOL_ERR_UNSUPPORTED;
   if (natoms < 0 || capacity <= 0 || ld < K.F) return FENNOL_ERR_INVALID;
@@ -892,16 +924,36 @@ extern "C" int fennol_aev_backward(const float* xyzs, int natoms, const int* ato
   if (bytes > 200 * 1024) return FENNOL_ERR_UNSUPPORTED;
   int blocks = (natoms + kAevWarps - 1) / kAevWarps;
   bool launched = dispatch(K, [&](auto ks) {
-    size_t smem = set_smem((const void*)ks.bwd, bytes);
+    auto fn = atom_virial ? ks.bwdv : ks.bwd;
+    size_t smem = set_smem((const void*)fn, bytes);
     if (!smem) return false;
-    ks.bwd<<<blocks, kAevWarps * 32, smem, (cudaStream_t)stream>>>(
+    fn<<<blocks, kAevWarps * 32, smem, (cudaStream_t)stream>>>(
         (const float4*)xyzs, natoms, atom_sys, sys_cell, nbr_j, nbr_shift, nbr_count, capacity, K,
-        atom_row, daev, ld, (float4*)forces4, status);
+        atom_row, daev, ld, (float4*)forces4, atom_virial, status);
     return true;
   });
   if (!launched) return FENNOL_ERR_UNSUPPORTED;
   FNL_CHECK_LAUNCH();
   return FENNOL_OK;
+}
+
+extern "C" int fennol_aev_backward(const float* xyzs, int natoms, const int* atom_sys,
+                                   const float* sys_cell, const int* nbr_j, const unsigned* nbr_shift,
+                                   const int* nbr_count, int capacity, const fennol_aev_params* p,
+                                   const int* atom_row, const float* daev, int ld, float* forces4,
+                                   int* status, void* stream) {
+  return aev_backward_launch(xyzs, natoms, atom_sys, sys_cell, nbr_j, nbr_shift, nbr_count, capacity, p,
+                             atom_row, daev, ld, forces4, nullptr, status, stream);
+}
+
+extern "C" int fennol_aev_backward_virial(const float* xyzs, int natoms, const int* atom_sys,
+                                          const float* sys_cell, const int* nbr_j, const unsigned* nbr_shift,
+                                          const int* nbr_count, int capacity, const fennol_aev_params* p,
+                                          const int* atom_row, const float* daev, int ld, float* forces4,
+                                          float* atom_virial, int* status, void* stream) {
+  if (natoms > 0 && !atom_virial) return FENNOL_ERR_INVALID;
+  return aev_backward_launch(xyzs, natoms, atom_sys, sys_cell, nbr_j, nbr_shift, nbr_count, capacity, p,
+                             atom_row, daev, ld, forces4, atom_virial, status, stream);
 }
 
 extern "C" int fennol_aev_tangent(const float* xyzs, int natoms, const int* atom_sys,

@@ -270,6 +270,40 @@ extern "C" size_t fennol_energy_workspace_bytes(int natoms, int nsys) {
   return 256 + (size_t)(nsys + 1) * sizeof(int) + 256 + chunks * sizeof(double);
 }
 
+// Per-system sum of per-centre virials, fixed order (one block per system).
+__global__ void __launch_bounds__(256) k_virial_reduce(const float* __restrict__ av,
+                                                       const int* __restrict__ sys_start, double scale,
+                                                       double* __restrict__ vir) {
+  __shared__ double red[9][256];
+  const int b = blockIdx.x, tid = threadIdx.x;
+  double acc[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) acc[q] = 0.0;
+  for (int i = sys_start[b] + tid; i < sys_start[b + 1]; i += 256)
+#pragma unroll
+    for (int q = 0; q < 9; ++q) acc[q] += (double)av[(size_t)i * 9 + q];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) red[q][tid] = acc[q];
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (tid < w)
+#pragma unroll
+      for (int q = 0; q < 9; ++q) red[q][tid] += red[q][tid + w];
+    __syncthreads();
+  }
+  if (tid < 9) vir[(size_t)b * 9 + tid] = scale * red[tid][0];
+}
+
+extern "C" int fennol_virial_reduce(const float* atom_virial, int natoms, const int* sys_start, int nsys,
+                                    double scale, double* virial, void* stream) {
+  if (natoms < 0 || nsys < 0) return FENNOL_ERR_INVALID;
+  if (nsys == 0) return FENNOL_OK;
+  if (!sys_start || !virial || (natoms > 0 && !atom_virial)) return FENNOL_ERR_INVALID;
+  k_virial_reduce<<<nsys, 256, 0, (cudaStream_t)stream>>>(atom_virial, sys_start, scale, virial);
+  FNL_CHECK_LAUNCH();
+  return FENNOL_OK;
+}
+
 extern "C" int fennol_energy_reduce(const float* e_rows, const int* atom_row, int natoms,
                                     const int* sys_start, int nsys, double scale, double* energy,
                                     double* e_atom, void* workspace, size_t workspace_bytes,

@@ -895,7 +895,8 @@ class FENNIX:
         self.preproc_state = state
         return out
 
-    def _evaluate(self, variables, inputs, want_forces: bool, want_embedding: bool = False):
+    def _evaluate(self, variables, inputs, want_forces: bool, want_embedding: bool = False,
+                  want_virial: bool = False):
         pot = self._potential(variables)
         layout: BatchLayout = inputs["_layout"]
         ws = self._workspace(pot, layout)
@@ -905,7 +906,7 @@ class FENNIX:
         call("fennol_pack_atoms", inputs["_coords"].data_ptr(), layout.t_species.data_ptr(), layout.n,
              ws.xyzs.data_ptr(), st)
         view = _RowsView(rows)
-        pot.launch_forces(layout, view, ws, st, want_forces)
+        pot.launch_forces(layout, view, ws, st, want_forces, want_virial)
         status = ws.status.cpu().numpy()
         if status[_lib.ST_ANG_OVERFLOW]:
             raise RuntimeError(f"more than {_lib.MAX_ANGULAR_NEIGHBORS} angular neighbours "
@@ -921,6 +922,9 @@ class FENNIX:
             call("fennol_forces_finalize", ws.forces4.data_ptr(), layout.n, 1.0, ws.forces.data_ptr(), st)
             f = ws.forces.clone()
             out["forces"] = f if self.energy_terms is not None else torch.zeros_like(f)
+        if want_virial:
+            vir = ws.virial.clone()
+            out["virial_tensor"] = vir if self.energy_terms is not None else torch.zeros_like(vir)
         if want_embedding:
             out[self.aev_module.embedding_key] = _embedding_from_rows(ws, layout,
                                                                        self.aev_config.aev_length)
@@ -955,8 +959,16 @@ class FENNIX:
         e, f = out["total_energy"] * fac, out["forces"] * fac
         return e, f, out
 
-    def energy_and_forces_and_virial(self, *args, **kwargs):
-        raise NotImplementedError("the virial is not computed by the CUDA adjoint")
+    def energy_and_forces_and_virial(self, variables=None, unit=None, gpu_preprocessing: bool = False,
+                                     **inputs):
+        """Energies, forces and ``virial_tensor`` [B, 3, 3] = dE/dS of the
+        deformation x -> x S, cell -> cell S at S = 1 (``fennix.py:320-347``)."""
+        if variables is None:
+            variables = self.variables
+        inputs = self.preprocess(use_gpu=gpu_preprocessing, **inputs)
+        out = self._evaluate(variables, inputs, want_forces=True, want_virial=True)
+        fac = self._unit_factor(unit)
+        return out["total_energy"] * fac, out["forces"] * fac, out["virial_tensor"] * fac, out
 
     def get_model(self):
         return (self.aev_module, self.net_module), self.variables

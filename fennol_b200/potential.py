@@ -320,6 +320,16 @@ class Workspace:
         ews = _lib.load().fennol_energy_workspace_bytes(layout.n, layout.nsys)
         self.energy_ws = torch.zeros(int(ews), dtype=torch.uint8, device=dev)
         self.status = torch.zeros(_lib.STATUS_WORDS, dtype=torch.int32, device=dev)
+        self.atom_virial = None
+        self.virial = None
+
+    def virial_buffers(self, layout: "BatchLayout"):
+        """Per-centre (float32 [N, 9]) and per-system (float64 [B, 3, 3]) virials."""
+        if self.atom_virial is None:
+            dev = layout.device
+            self.atom_virial = torch.zeros((max(layout.n, 1), 9), dtype=torch.float32, device=dev)
+            self.virial = torch.zeros((layout.nsys, 3, 3), dtype=torch.float64, device=dev)
+        return self.atom_virial, self.virial
 
 
 class ANIPotential:
@@ -411,7 +421,7 @@ class ANIPotential:
 
     # --------------------------------------------------------------- launches
     def launch_forces(self, layout: BatchLayout, g: GraphBuffers, ws: Workspace, stream: int,
-                      want_forces: bool = True):
+                      want_forces: bool = True, want_virial: bool = False):
         """AEV -> MLP -> energies (and adjoint -> forces) from the current radial list."""
         lib_p = C_ptr(self.params)
         n = layout.n
@@ -426,7 +436,16 @@ class ANIPotential:
         call("fennol_energy_reduce", ws.e_rows.data_ptr(), layout.t_atom_row.data_ptr(), n,
              layout.t_sys_start.data_ptr(), layout.nsys, float(self.unit_scale), ws.energy.data_ptr(),
              ws.e_atom.data_ptr(), ws.energy_ws.data_ptr(), ws.energy_ws.numel(), stream)
-        if want_forces:
+        if want_forces and want_virial:
+            ws.forces4.zero_()
+            av, vir = ws.virial_buffers(layout)
+            call("fennol_aev_backward_virial", ws.xyzs.data_ptr(), n, layout.t_atom_sys.data_ptr(),
+                 layout.t_cell.data_ptr(), g.rad_j.data_ptr(), g.rad_s.data_ptr(), g.rad_n.data_ptr(),
+                 g.cap_r, lib_p, layout.t_atom_row.data_ptr(), ws.dx.data_ptr(), ws.dx.shape[1],
+                 ws.forces4.data_ptr(), av.data_ptr(), ws.status.data_ptr(), stream)
+            call("fennol_virial_reduce", av.data_ptr(), n, layout.t_sys_start.data_ptr(), layout.nsys,
+                 float(self.unit_scale), vir.data_ptr(), stream)
+        elif want_forces:
             ws.forces4.zero_()
             call("fennol_aev_backward", ws.xyzs.data_ptr(), n, layout.t_atom_sys.data_ptr(),
                  layout.t_cell.data_ptr(), g.rad_j.data_ptr(), g.rad_s.data_ptr(), g.rad_n.data_ptr(),
@@ -467,6 +486,17 @@ class ANIPotential:
         """Energies [B] (float64) and forces [N,3] (float32) as torch tensors
         on the device.  ``coordinates`` may be a host array or a device
         tensor ([N,3], Angstrom); ``species`` are atomic numbers."""
+        ws = self._evaluate(coordinates, species, natoms, cells, want_forces, False)
+        return ws.energy, (ws.forces if want_forces else None)
+
+    def energy_forces_virial(self, coordinates, species, natoms=None, cells=None):
+        """Energies [B], forces [N,3] and the virial tensor [B,3,3] (float64):
+        dE/dS of the deformation x -> x S, cell -> cell S at S = 1, FeNNol's
+        ``virial_tensor`` (``fennix.py:320-347``), in the energy unit."""
+        ws = self._evaluate(coordinates, species, natoms, cells, True, True)
+        return ws.energy, ws.forces, ws.virial
+
+    def _evaluate(self, coordinates, species, natoms, cells, want_forces: bool, want_virial: bool):
         species = np.asarray(species)
         if natoms is None:
             natoms = [species.shape[0]]
@@ -484,7 +514,7 @@ class ANIPotential:
             coords = coords.to(self.device, non_blocking=True)
         coords = coords.contiguous()
         stream = _stream(self.device)
-        gkey = (key, bool(want_forces))
+        gkey = (key, bool(want_forces), bool(want_virial))
         rec = self._graphs.get(gkey) if self.use_graphs else None
         if rec is not None and rec["g"] is g:
             # same batch as the last calls: one graph launch for the whole evaluation
@@ -492,12 +522,12 @@ class ANIPotential:
             rec["graph"].replay()
             grow = self.check_status(ws, g)
             if grow is None:
-                return ws.energy, (ws.forces if want_forces else None)
+                return ws
             self._graphs.pop(gkey, None)
             g = GraphBuffers(layout, g.cutoff, g.skin, grow[0], grow[1])
             self._cache[key] = (layout, g, ws)
         for _attempt in range(4):
-            self._launch_all(layout, g, ws, coords, stream, want_forces)
+            self._launch_all(layout, g, ws, coords, stream, want_forces, want_virial)
             grow = self.check_status(ws, g)
             if grow is None:
                 break
@@ -509,11 +539,11 @@ class ANIPotential:
             calls = self._calls.get(gkey, 0) + 1
             self._calls = {gkey: calls}
             if calls >= 2:  # a repeated batch: capture it once
-                self._capture(gkey, layout, g, ws, coords, want_forces)
-        return ws.energy, (ws.forces if want_forces else None)
+                self._capture(gkey, layout, g, ws, coords, want_forces, want_virial)
+        return ws
 
     def _launch_all(self, layout: BatchLayout, g: GraphBuffers, ws: Workspace, coords: torch.Tensor,
-                    stream: int, want_forces: bool):
+                    stream: int, want_forces: bool, want_virial: bool = False):
         """Every launch of one evaluation: pack, list build and filter, AEV,
         MLP, energy sum, adjoint and force finalisation."""
         ws.status.zero_()
@@ -521,17 +551,17 @@ class ANIPotential:
              ws.xyzs.data_ptr(), stream)
         g.build(layout, coords, ws.status, stream)
         g.filter(layout, coords, ws.status, stream)
-        self.launch_forces(layout, g, ws, stream, want_forces)
+        self.launch_forces(layout, g, ws, stream, want_forces, want_virial)
         if want_forces:
             call("fennol_forces_finalize", ws.forces4.data_ptr(), layout.n, float(self.unit_scale),
                  ws.forces.data_ptr(), stream)
 
-    def _capture(self, gkey, layout, g, ws, coords, want_forces):
+    def _capture(self, gkey, layout, g, ws, coords, want_forces, want_virial):
         buf = torch.empty_like(coords)
         buf.copy_(coords)
         graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(graph):
-            self._launch_all(layout, g, ws, buf, _stream(self.device), want_forces)
+            self._launch_all(layout, g, ws, buf, _stream(self.device), want_forces, want_virial)
         self._graphs = {gkey: {"graph": graph, "coords": buf, "g": g}}
         # the replay recomputes the same values; results of this call stay valid
 

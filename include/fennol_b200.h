@@ -212,6 +212,19 @@ int fennol_aev_backward(const float* xyzs, int natoms, const int* atom_sys,
                         int* status, void* stream);
 
 /*
+ * fennol_aev_backward that also writes, per centre atom i, the 3x3 sum over
+ * its edges of r_ij (x) dE/dr_ij (atom_virial, float32 [natoms*9], row-major
+ * a,b = r_a * g_b).  Summed per system (fennol_virial_reduce) this is the
+ * reference's virial_tensor = dE/dS of a homogeneous deformation
+ * x -> x S, cell -> cell S at S = 1 (fennix.py:320-347).
+ */
+int fennol_aev_backward_virial(const float* xyzs, int natoms, const int* atom_sys,
+                               const float* sys_cell, const int* nbr_j, const unsigned* nbr_shift,
+                               const int* nbr_count, int capacity, const fennol_aev_params* p,
+                               const int* atom_row, const float* daev, int ld, float* forces4,
+                               float* atom_virial, int* status, void* stream);
+
+/*
  * Forward-mode tangent of the AEV: out[atom_row[i]*ld + f] = sum_k
  * dAEV_i,f/dx_k . du_k for a displacement field du4 (float32 [natoms*4],
  * x, y, z, unused).  No counterpart call in the reference: jax.grad over a
@@ -303,6 +316,11 @@ int fennol_energy_reduce(const float* e_rows, const int* atom_row, int natoms,
 /* forces[i*3+k] = scale * forces4[i*4+k] (float32 output). */
 int fennol_forces_finalize(const float* forces4, int natoms, float scale, float* forces,
                            void* stream);
+
+/* virial[b*9 + k] = scale * sum of atom_virial[i*9 + k] over the atoms of
+ * system b (float64, fixed order). */
+int fennol_virial_reduce(const float* atom_virial, int natoms, const int* sys_start, int nsys,
+                         double scale, double* virial, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Molecular dynamics                                                        */

@@ -78,8 +78,11 @@ def _switch(d, mask, rc):
     return torch.where(mask, 0.5 * torch.cos(d * (math.pi / rc)) + 0.5, torch.zeros_like(d))
 
 
-def aev(coords: torch.Tensor, species_idx: np.ndarray, g: Graph, cfg) -> torch.Tensor:
-    """ANIAEV embedding ``[nat, F]`` (ani.py:47-139)."""
+def aev(coords: torch.Tensor, species_idx: np.ndarray, g: Graph, cfg,
+        strain: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """ANIAEV embedding ``[nat, F]`` (ani.py:47-139).  ``strain`` ([B,3,3]):
+    every edge vector of system b becomes ``vec @ strain[b]`` (the homogeneous
+    deformation the reference differentiates for the virial, fennix.py:320-347)."""
     dt = coords.dtype
     nat = coords.shape[0]
     S = cfg.num_species
@@ -94,6 +97,8 @@ def aev(coords: torch.Tensor, species_idx: np.ndarray, g: Graph, cfg) -> torch.T
         else:
             cb = torch.as_tensor(g.cells, dtype=dt)[torch.as_tensor(g.batch_index)[src]]
             vec = vec + torch.einsum("ej,eji->ei", sh, cb)
+    if strain is not None:
+        vec = torch.einsum("ej,ejk->ek", vec, strain[torch.as_tensor(g.batch_index)[src]])
     d2 = (vec ** 2).sum(-1)
     dist = torch.sqrt(torch.clamp(d2, min=1e-5))
     rc = g.radial_cutoff
@@ -245,3 +250,25 @@ def loss_value(coordinates, species, natoms, model: Dict, aev_cfg, mlp_cfg, e_re
     e = np.asarray(r["energy"]) - np.asarray(e_ref, np.float64)
     f = np.asarray(r["forces"]) - np.asarray(f_ref, np.float64).reshape(r["forces"].shape)
     return float(w_e * np.mean(e ** 2) + w_f * np.mean(f ** 2))
+
+
+def energy_forces_virial(coordinates, species, natoms, weights: List[Dict], aev_cfg, mlp_cfg,
+                         cells=None, minimum_image=True, dtype=torch.float64):
+    """Energies, forces and the reference's ``virial_tensor`` = dE/dS at S = 1
+    for x -> x S, cell -> cell S per system (fennix.py:320-347), FP64 autograd."""
+    coordinates = np.asarray(coordinates, dtype=np.float64)
+    natoms = np.asarray(natoms).reshape(-1)
+    graph = Graph(coordinates, natoms, cells, None, aev_cfg.radial_cutoff, aev_cfg.angular_cutoff,
+                  minimum_image)
+    sidx = aev_cfg.species_index(species)
+    x = torch.tensor(coordinates, dtype=dtype, requires_grad=True)
+    S = torch.eye(3, dtype=dtype).repeat(natoms.shape[0], 1, 1).requires_grad_(True)
+    emb = aev(x, sidx, graph, aev_cfg, strain=S)
+    eat = None
+    for model in weights:
+        e = species_net(emb, sidx, model, aev_cfg.species_order, mlp_cfg.celu_alpha)
+        eat = e if eat is None else eat + e
+    eat = eat / len(weights)
+    etot = torch.zeros(natoms.shape[0], dtype=dtype).index_add(0, torch.as_tensor(graph.batch_index), eat)
+    gx, gs = torch.autograd.grad(etot.sum(), (x, S))
+    return {"energy": etot.detach().numpy(), "forces": (-gx).numpy(), "virial": gs.numpy()}

@@ -189,3 +189,22 @@ def test_loss_parameter_gradients_match_finite_differences():
         fd = (lp - lm) / (2 * h)
         g = grads[sym][layer][which][idx]
         assert abs(fd - g) <= 1e-5 * abs(g) + 1e-9 * max(1.0, loss), (sym, layer, which, idx, fd, g)
+
+
+def test_virial_of_a_molecule_is_minus_sum_x_outer_f():
+    """Without a cell the strain derivative equals sum_i x_i (x) dE/dx_i."""
+    from fennol_b200.params import AEVConfig, MLPConfig, init_weights
+    from fennol_b200.systems import molecule_batch
+    from oracle import ani_ref
+
+    cfg, mcfg = AEVConfig(), MLPConfig()
+    mols = molecule_batch(2, seed=17, nmin=10, nmax=16)
+    xyz = np.concatenate([m.coordinates for m in mols])
+    sp = np.concatenate([m.species for m in mols])
+    nat = [m.natoms for m in mols]
+    W = init_weights(cfg, mcfg, seed=2)
+    r = ani_ref.energy_forces_virial(xyz, sp, nat, W, cfg, mcfg)
+    off = np.concatenate([[0], np.cumsum(nat)])
+    for b in range(len(nat)):
+        x, f = xyz[off[b]:off[b + 1]], r["forces"][off[b]:off[b + 1]]
+        np.testing.assert_allclose(r["virial"][b], -np.einsum("ia,ib->ab", x, f), rtol=1e-10, atol=1e-12)
