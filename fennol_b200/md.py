@@ -55,6 +55,8 @@ class MDEngine:
         dev = pot.device
         self.device = dev
         species = np.asarray(species)
+        self.species = species
+        self.cell = None if cell is None else np.asarray(cell, dtype=np.float64)
         coordinates = np.asarray(coordinates, dtype=np.float64)
         natoms = [species.shape[0]] if natoms is None else list(natoms)
         cells = None if cell is None else np.asarray(cell).reshape(-1, 3, 3)
@@ -234,6 +236,28 @@ class MDEngine:
             self.snapshot()
         if sync:
             torch.cuda.synchronize(self.device)
+
+    def run_with_frames(self, nsteps: int, every: int, frames, graph_steps: int = 1):
+        """Advance ``nsteps`` steps and queue the positions every ``every``
+        steps into ``frames`` (a :class:`fennol_b200.trajectory.FrameStream`);
+        the copies overlap the following steps."""
+        done = 0
+        while done < nsteps:
+            k = min(every, nsteps - done)
+            self.run(k, graph_steps=graph_steps, sync=False)
+            done += k
+            if done % every == 0:
+                frames.push(self.x, properties={"time_ps": f"{self.simulation_time_ps():.6f}"})
+        torch.cuda.synchronize(self.device)
+
+    def simulation_time_ps(self) -> float:
+        return self.step_count * self.dt
+
+    def save_restart(self, path: str):
+        """Positions, velocities and time in the reference's restart layout."""
+        from .trajectory import save_restart
+        save_restart(path, self.species, self.x.cpu().numpy(), self.v.cpu().numpy(),
+                     self.simulation_time_ps(), self.cell)
 
     # ------------------------------------------------------------ observables
     def potential_energy(self) -> float:
