@@ -1,5 +1,13 @@
 """Benchmark of the ANI-2x energy+force MD step on B200.
 
+The JSON line also carries: per-kernel rooflines (``kernels``), the FP32
+form on the same workload, accuracy against the FP64 oracle, the end-to-end
+public-API call with host buffers (``e2e``), the CPU oracle on the host
+cores (``cpu_baseline``), a Poisson request stream through the serving loop
+(``serving``), the training-loss gradient of a 256-molecule batch
+(``training_256mol``), the 98,304-atom 8-model ensemble against its FP32 form
+(``ensemble_98k``) and, with ``--nve-drift-steps``, the NVE energy drift.
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload water12k|water98k] [--precision bf16x3|bf16x2|bf16|fp32]
 
@@ -599,14 +607,15 @@ def main():
                                                    "rounded to BF16 (same weights in the oracle)")
         del spec
         res["e2e"] = e2e(pot, box, max(5, args.steps // 3), 3)
-        if not args.skip_98k and args.workload != "water98k":
-            del eng, pot
-            torch.cuda.empty_cache()
-            res["ensemble_98k"] = ensemble_98k(device, 5, 3, flush)
         if not args.skip_serving:
             res["serving"] = serving_run(device)
         if not args.skip_training:
             res["training_256mol"] = training_256(device)
+        if not args.skip_98k and args.workload != "water98k":
+            # last: the 98k-atom engines hold several GB that later parts would work around
+            del eng, pot
+            torch.cuda.empty_cache()
+            res["ensemble_98k"] = ensemble_98k(device, 5, 3, flush)
         if args.nve_drift_steps > 0:
             res["nve_drift"] = nve_drift(device, args.nve_drift_steps)
         if not args.no_cpu_baseline:
