@@ -310,7 +310,7 @@ extern "C" int fennol_energy_reduce(const float* e_rows, const int* atom_row, in
                                     void* stream) {
   if (natoms < 0 || nsys < 0) return FENNOL_ERR_INVALID;
   if (nsys == 0) return FENNOL_OK;
-  if (!e_rows || !atom_row || !sys_start || !energy || !workspace) return FENNOL_ERR_INVALID;
+  if (!sys_start || !energy || !workspace || (natoms > 0 && (!e_rows || !atom_row))) return FENNOL_ERR_INVALID;
   if (workspace_bytes < fennol_energy_workspace_bytes(natoms, nsys)) return FENNOL_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   int* chunk_off = (int*)workspace;

@@ -487,14 +487,16 @@ class ANIPotential:
         on the device.  ``coordinates`` may be a host array or a device
         tensor ([N,3], Angstrom); ``species`` are atomic numbers."""
         ws = self._evaluate(coordinates, species, natoms, cells, want_forces, False)
-        return ws.energy, (ws.forces if want_forces else None)
+        n = self._cache[next(iter(self._cache))][0].n
+        return ws.energy, (ws.forces[:n] if want_forces else None)
 
     def energy_forces_virial(self, coordinates, species, natoms=None, cells=None):
         """Energies [B], forces [N,3] and the virial tensor [B,3,3] (float64):
         dE/dS of the deformation x -> x S, cell -> cell S at S = 1, FeNNol's
         ``virial_tensor`` (``fennix.py:320-347``), in the energy unit."""
         ws = self._evaluate(coordinates, species, natoms, cells, True, True)
-        return ws.energy, ws.forces, ws.virial
+        n = self._cache[next(iter(self._cache))][0].n
+        return ws.energy, ws.forces[:n], ws.virial
 
     def _evaluate(self, coordinates, species, natoms, cells, want_forces: bool, want_virial: bool):
         species = np.asarray(species)
