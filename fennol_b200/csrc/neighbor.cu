@@ -17,7 +17,7 @@ using namespace fnl;
 namespace {
 
 constexpr int kBuildWarps = 4;      // warps per block in the row builders
-constexpr int kMaxSortRow = 1024;   // largest row the in-smem sort handles
+constexpr int kMaxRow = 1024;       // longest neighbour row accepted
 
 struct SysView {
   const int* start;
@@ -27,8 +27,6 @@ struct SysView {
   const int* grid;
   const int* nrep;
 };
-
-__device__ __forceinline__ size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 struct GraphWs {
   int* counts;      // [C]
@@ -155,8 +153,8 @@ __global__ void k_scan(GraphWs w, int c, const int* enable_flag) {
   if (tid == 0) w.starts[c] = carry;
 }
 
-// 3. scatter atoms into their cells (order inside a cell is arbitrary; rows are
-//    sorted afterwards so the final lists are deterministic).
+// 3. scatter atoms into their cells (order inside a cell is arbitrary until
+//    k_sort_cells puts each cell in increasing index order).
 __global__ void k_scatter(int n, GraphWs w, const int* enable_flag) {
   if (enable_flag && *enable_flag == 0) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -198,122 +196,157 @@ __device__ __forceinline__ bool pair_test(int mode, float4 pi, float4 pj, unsign
   return d2 < rc2;
 }
 
-// Bitonic sort of `m` (power of two) 64-bit keys in shared memory by one warp.
-__device__ void warp_bitonic_sort(unsigned long long* keys, int m, int lane) {
+// Append the candidates selected by `keep` (one per lane) to row `base` in
+// global memory, in lane order after the `count` entries already there.
+__device__ __forceinline__ void row_append(bool keep, int j, unsigned sh, int* __restrict__ nbr_j,
+                                           unsigned* __restrict__ nbr_shift, size_t base, int cap, int& count,
+                                           int lane) {
+  const unsigned m = __ballot_sync(0xffffffffu, keep);
+  if (keep) {
+    const int pos = count + warp_exclusive_prefix(m, lane);
+    if (pos < cap) {
+      nbr_j[base + pos] = j;
+      nbr_shift[base + pos] = sh;
+    }
+  }
+  count += __popc(m);
+}
+
+__device__ __forceinline__ void row_finish(int i, int count, int cap, int* __restrict__ nbr_count, int* status,
+                                           int lane) {
+  if (lane == 0) {
+    nbr_count[i] = count < cap ? count : cap;
+    if (count > cap) status_set(status, ST_NBR_OVERFLOW);
+    status_max(status, ST_NBR_MAXCOUNT, count);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 3b. each cell's atom list in increasing index order (warp per cell), so
+//     that rows built in stencil order are deterministic.
+// ---------------------------------------------------------------------------
+constexpr int kCellSortMax = 512;  // larger cells (densities far above a liquid's) keep scatter order
+
+__global__ void __launch_bounds__(256) k_sort_cells(int c, GraphWs w, const int* enable_flag) {
+  if (enable_flag && *enable_flag == 0) return;
+  __shared__ int buf[8][kCellSortMax];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int cell = blockIdx.x * 8 + warp;
+  if (cell >= c) return;
+  const int s0 = w.starts[cell], n = w.starts[cell + 1] - s0;
+  if (n <= 1) return;
+  if (n <= 32) {
+    int v = lane < n ? w.cell_atoms[s0 + lane] : 0x7fffffff;
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        const int o = __shfl_xor_sync(0xffffffffu, v, j);
+        const bool up = (lane & k) == 0, lower = (lane & j) == 0;
+        v = (lower == up) ? min(v, o) : max(v, o);
+      }
+    }
+    if (lane < n) w.cell_atoms[s0 + lane] = v;
+    return;
+  }
+  if (n > kCellSortMax) return;
+  int m = 64;
+  while (m < n) m <<= 1;
+  int* b = buf[warp];
+  for (int k = lane; k < m; k += 32) b[k] = k < n ? w.cell_atoms[s0 + k] : 0x7fffffff;
+  __syncwarp();
   for (int k = 2; k <= m; k <<= 1) {
     for (int j = k >> 1; j > 0; j >>= 1) {
       for (int idx = lane; idx < m; idx += 32) {
-        int ixj = idx ^ j;
+        const int ixj = idx ^ j;
         if (ixj > idx) {
-          unsigned long long a = keys[idx], b = keys[ixj];
-          bool up = (idx & k) == 0;
-          if ((a > b) == up) {
-            keys[idx] = b;
-            keys[ixj] = a;
+          const int a = b[idx], bb = b[ixj];
+          if ((a > bb) == ((idx & k) == 0)) {
+            b[idx] = bb;
+            b[ixj] = a;
           }
         }
       }
       __syncwarp();
     }
   }
-}
-
-__device__ __forceinline__ unsigned long long make_key(int j, unsigned shift) {
-  return ((unsigned long long)(unsigned)j << 32) | (unsigned long long)shift;
-}
-
-// Append candidates selected by `keep` (one per lane) to the warp's key row.
-__device__ __forceinline__ void warp_append(bool keep, int j, unsigned shift, unsigned long long* keys,
-                                            int cap, int& count, int lane) {
-  unsigned m = __ballot_sync(0xffffffffu, keep);
-  if (keep) {
-    int pos = count + warp_exclusive_prefix(m, lane);
-    if (pos < cap) keys[pos] = make_key(j, shift);
-  }
-  count += __popc(m);
-}
-
-__device__ void finish_row(int i, unsigned long long* keys, int count, int cap, int sort_len,
-                           int* __restrict__ nbr_j, unsigned* __restrict__ nbr_shift,
-                           int* __restrict__ nbr_count, int* status, int lane) {
-  int stored = count < cap ? count : cap;
-  if (count > cap) {
-    if (lane == 0) {
-      status_set(status, ST_NBR_OVERFLOW);
-    }
-  }
-  if (lane == 0) status_max(status, ST_NBR_MAXCOUNT, count);
-  // pad and sort the stored part
-  int m = 1;
-  while (m < stored) m <<= 1;
-  if (m > sort_len) m = sort_len;
-  for (int k = stored + lane; k < m; k += 32) keys[k] = ~0ull;
-  __syncwarp();
-  if (stored > 1) warp_bitonic_sort(keys, m, lane);
-  size_t base = (size_t)i * cap;
-  for (int k = lane; k < stored; k += 32) {
-    unsigned long long key = keys[k];
-    nbr_j[base + k] = (int)(key >> 32);
-    nbr_shift[base + k] = (unsigned)(key & 0xFFFFFFFFull);
-  }
-  if (lane == 0) nbr_count[i] = stored;
-  __syncwarp();
+  for (int k = lane; k < n; k += 32) w.cell_atoms[s0 + k] = b[k];
 }
 
 // ---------------------------------------------------------------------------
-// 4a. cell-list rows: one warp per atom, 27 stencil cells, ballot compaction.
+// 4a. cell-list rows: one warp per atom.  The 27 stencil cells' atom ranges
+//     are concatenated, so every 32-lane round tests 32 candidates whatever
+//     the cell sizes; kept pairs go straight to the row in candidate order
+//     (stencil cell, then atom index), which makes the rows deterministic.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kBuildWarps * 32)
 k_build_cells(int n, const int* __restrict__ atom_sys, SysView sv, GraphWs w, float rc2, int cap,
-              int sort_len, int* __restrict__ nbr_j, unsigned* __restrict__ nbr_shift,
-              int* __restrict__ nbr_count, int* status, const int* enable_flag) {
+              int* __restrict__ nbr_j, unsigned* __restrict__ nbr_shift, int* __restrict__ nbr_count,
+              int* status, const int* enable_flag) {
   if (enable_flag && *enable_flag == 0) return;
-  extern __shared__ unsigned long long smem_keys[];
-  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int i = blockIdx.x * kBuildWarps + warp;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i = blockIdx.x * kBuildWarps + warp;
   if (i >= n) return;
-  int cell = w.atom_cell[i];
+  const int cell = w.atom_cell[i];
   if (cell < 0) return;  // all-pairs system
-  unsigned long long* keys = smem_keys + (size_t)warp * sort_len;
-  int b = atom_sys[i];
-  int mode = sv.mode[b];
+  const int b = atom_sys[i];
+  const int mode = sv.mode[b];
   const float* c = sv.cell + 9 * b;
   const float* r = sv.recip + 9 * b;
   const int* g = sv.grid + 4 * b;
-  int nx = g[0], ny = g[1], nz = g[2], off = g[3];
-  int local = cell - off;
-  int cz = local % nz, cy = (local / nz) % ny, cx = local / (ny * nz);
-  float4 pi = w.pos[i];
-  unsigned ati = w.at[i];
-  int count = 0;
-  for (int dx = -1; dx <= 1; ++dx) {
-    int ex = cx + dx, wx = 0;
+  const int nx = g[0], ny = g[1], nz = g[2], off = g[3];
+  const int local = cell - off;
+  const int cz = local % nz, cy = (local / nz) % ny, cx = local / (ny * nz);
+  // lane s < 27: stencil cell s = (dx, dy, dz) + 1 in base 3, its atom range and wrap
+  int s0 = 0, cnt = 0, wrap = 0;
+  if (lane < 27) {
+    int ex = cx + lane / 9 - 1, ey = cy + (lane / 3) % 3 - 1, ez = cz + lane % 3 - 1;
+    int wx = 0, wy = 0, wz = 0;
     if (ex < 0) { ex += nx; wx = -1; } else if (ex >= nx) { ex -= nx; wx = 1; }
-    for (int dy = -1; dy <= 1; ++dy) {
-      int ey = cy + dy, wy = 0;
-      if (ey < 0) { ey += ny; wy = -1; } else if (ey >= ny) { ey -= ny; wy = 1; }
-      for (int dz = -1; dz <= 1; ++dz) {
-        int ez = cz + dz, wz = 0;
-        if (ez < 0) { ez += nz; wz = -1; } else if (ez >= nz) { ez -= nz; wz = 1; }
-        int nc = off + (ex * ny + ey) * nz + ez;
-        int s0 = w.starts[nc], s1 = w.starts[nc + 1];
-        for (int k0 = s0; k0 < s1; k0 += 32) {
-          int k = k0 + lane;
-          bool keep = false;
-          int j = -1;
-          unsigned sh = 0;
-          if (k < s1) {
-            j = w.cell_atoms[k];
-            if (j != i)
-              keep = pair_test(mode, pi, w.pos[j], ati, w.at[j], wx, wy, wz, c, r, rc2, sh);
-          }
-          warp_append(keep, j, sh, keys, cap, count, lane);
-        }
-      }
-    }
+    if (ey < 0) { ey += ny; wy = -1; } else if (ey >= ny) { ey -= ny; wy = 1; }
+    if (ez < 0) { ez += nz; wz = -1; } else if (ez >= nz) { ez -= nz; wz = 1; }
+    const int nc = off + (ex * ny + ey) * nz + ez;
+    s0 = w.starts[nc];
+    cnt = w.starts[nc + 1] - s0;
+    wrap = (wx + 1) | ((wy + 1) << 2) | ((wz + 1) << 4);
   }
-  __syncwarp();
-  finish_row(i, keys, count, cap, sort_len, nbr_j, nbr_shift, nbr_count, status, lane);
+  int incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  const int first = incl - cnt;  // first candidate of stencil cell `lane`
+  const int total = __shfl_sync(0xffffffffu, incl, 31);
+  const float4 pi = w.pos[i];
+  const unsigned ati = w.at[i];
+  const size_t base = (size_t)i * cap;
+  int count = 0;
+  for (int k0 = 0; k0 < total; k0 += 32) {
+    const int k = k0 + lane;
+    // stencil cell of candidate k: the last s < 27 with first[s] <= k
+    int sc = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1) {
+      const int cand = sc + step;
+      const int fc = __shfl_sync(0xffffffffu, first, cand & 31);
+      if (cand < 27 && fc <= k) sc = cand;
+    }
+    const int sfirst = __shfl_sync(0xffffffffu, first, sc);
+    const int sstart = __shfl_sync(0xffffffffu, s0, sc);
+    const int swrap = __shfl_sync(0xffffffffu, wrap, sc);
+    bool keep = false;
+    int j = -1;
+    unsigned sh = 0;
+    if (k < total) {
+      j = w.cell_atoms[sstart + k - sfirst];
+      if (j != i)
+        keep = pair_test(mode, pi, w.pos[j], ati, w.at[j], (swrap & 3) - 1, ((swrap >> 2) & 3) - 1,
+                         ((swrap >> 4) & 3) - 1, c, r, rc2, sh);
+    }
+    row_append(keep, j, sh, nbr_j, nbr_shift, base, cap, count, lane);
+  }
+  row_finish(i, count, cap, nbr_count, status, lane);
 }
 
 // ---------------------------------------------------------------------------
@@ -321,15 +354,14 @@ k_build_cells(int n, const int* __restrict__ atom_sys, SysView sv, GraphWs w, fl
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kBuildWarps * 32)
 k_build_allpairs(int n, const int* __restrict__ atom_sys, SysView sv, GraphWs w, float rc2, int cap,
-                 int sort_len, int* __restrict__ nbr_j, unsigned* __restrict__ nbr_shift,
-                 int* __restrict__ nbr_count, int* status, const int* enable_flag) {
+                 int* __restrict__ nbr_j, unsigned* __restrict__ nbr_shift, int* __restrict__ nbr_count,
+                 int* status, const int* enable_flag) {
   if (enable_flag && *enable_flag == 0) return;
-  extern __shared__ unsigned long long smem_keys[];
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int i = blockIdx.x * kBuildWarps + warp;
   if (i >= n) return;
   if (w.atom_cell[i] >= 0) return;  // cell-list system
-  unsigned long long* keys = smem_keys + (size_t)warp * sort_len;
+  const size_t base = (size_t)i * cap;
   int b = atom_sys[i];
   int mode = sv.mode[b];
   const float* c = sv.cell + 9 * b;
@@ -353,11 +385,10 @@ k_build_allpairs(int n, const int* __restrict__ atom_sys, SysView sv, GraphWs w,
           unsigned sh = 0;
           if (j < j1 && j != i)
             keep = pair_test(mode, pi, w.pos[j], ati, w.at[j], ix, iy, iz, c, r, rc2, sh);
-          warp_append(keep, j, sh, keys, cap, count, lane);
+          row_append(keep, j, sh, nbr_j, nbr_shift, base, cap, count, lane);
         }
       }
-  __syncwarp();
-  finish_row(i, keys, count, cap, sort_len, nbr_j, nbr_shift, nbr_count, status, lane);
+  row_finish(i, count, cap, nbr_count, status, lane);
 }
 
 __global__ void k_count_rebuild(int* status, const int* enable_flag) {
@@ -466,11 +497,6 @@ extern "C" size_t fennol_graph_workspace_bytes(int natoms, int ncells_total) {
   return ws_layout(natoms, ncells_total, nullptr, nullptr);
 }
 
-static int sort_len_for(int cap) {
-  int m = 1;
-  while (m < cap) m <<= 1;
-  return m;
-}
 
 extern "C" int fennol_graph_build(const float* coords, int natoms, const int* atom_sys, int nsys,
                                   const int* sys_start, const int* sys_mode, const float* sys_cell,
@@ -478,7 +504,7 @@ extern "C" int fennol_graph_build(const float* coords, int natoms, const int* at
                                   int ncells_total, double cutoff, int capacity, int* nbr_j,
                                   unsigned* nbr_shift, int* nbr_count, int* status, void* workspace,
                                   size_t workspace_bytes, const int* enable_flag, void* stream) {
-  if (natoms < 0 || nsys <= 0 || capacity <= 0 || capacity > kMaxSortRow || !(cutoff > 0))
+  if (natoms < 0 || nsys <= 0 || capacity <= 0 || capacity > kMaxRow || !(cutoff > 0))
     return FENNOL_ERR_INVALID;
   if (natoms == 0) return FENNOL_OK;
   if (!coords || !atom_sys || !sys_start || !sys_mode || !sys_grid || !sys_nrep || !nbr_j ||
@@ -490,15 +516,6 @@ extern "C" int fennol_graph_build(const float* coords, int natoms, const int* at
   ws_layout(natoms, ncells_total, (char*)workspace, &w);
   SysView sv{sys_start, sys_mode, sys_cell, sys_recip, sys_grid, sys_nrep};
   float rc2 = (float)(cutoff * cutoff);
-  int sort_len = sort_len_for(capacity);
-  size_t smem = (size_t)kBuildWarps * sort_len * sizeof(unsigned long long);
-  if (smem > 48 * 1024) {
-    if (cudaFuncSetAttribute(k_build_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-            cudaSuccess ||
-        cudaFuncSetAttribute(k_build_allpairs, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess)
-      return FENNOL_ERR_CUDA;
-  }
   if (ncells_total > 0) {
     if (cudaMemsetAsync(w.counts, 0, sizeof(int) * (size_t)ncells_total, st) != cudaSuccess)
       return FENNOL_ERR_CUDA;
@@ -512,15 +529,17 @@ extern "C" int fennol_graph_build(const float* coords, int natoms, const int* at
     FNL_CHECK_LAUNCH();
     k_scatter<<<gb, tb, 0, st>>>(natoms, w, enable_flag);
     FNL_CHECK_LAUNCH();
+    k_sort_cells<<<(ncells_total + 7) / 8, 256, 0, st>>>(ncells_total, w, enable_flag);
+    FNL_CHECK_LAUNCH();
   }
   int gw = (natoms + kBuildWarps - 1) / kBuildWarps;
   if (ncells_total > 0) {
-    k_build_cells<<<gw, kBuildWarps * 32, smem, st>>>(natoms, atom_sys, sv, w, rc2, capacity, sort_len,
-                                                       nbr_j, nbr_shift, nbr_count, status, enable_flag);
+    k_build_cells<<<gw, kBuildWarps * 32, 0, st>>>(natoms, atom_sys, sv, w, rc2, capacity, nbr_j, nbr_shift,
+                                                    nbr_count, status, enable_flag);
     FNL_CHECK_LAUNCH();
   }
-  k_build_allpairs<<<gw, kBuildWarps * 32, smem, st>>>(natoms, atom_sys, sv, w, rc2, capacity, sort_len,
-                                                        nbr_j, nbr_shift, nbr_count, status, enable_flag);
+  k_build_allpairs<<<gw, kBuildWarps * 32, 0, st>>>(natoms, atom_sys, sv, w, rc2, capacity, nbr_j, nbr_shift,
+                                                     nbr_count, status, enable_flag);
   FNL_CHECK_LAUNCH();
   if (status) {
     k_count_rebuild<<<1, 1, 0, st>>>(status, enable_flag);
