@@ -376,7 +376,6 @@ class ANIPotential:
         self._cache: Dict[tuple, tuple] = {}
         self.capacity_margin = 1.05
         self.add_neigh = 8
-        self._tc_launches = 6
         # repeated calls on the same batch replay one captured CUDA graph
         self.use_graphs = use_graphs
         self._graphs: Dict[tuple, dict] = {}
@@ -414,10 +413,15 @@ class ANIPotential:
         return g, ws
 
     def mlp_launches(self) -> int:
-        """Kernels launched by one fennol_mlp_energy_grad call."""
+        """Kernels launched by one fennol_mlp_energy_grad call: the FP32 form
+        runs 7 per model, the fused tcgen05 kernel (BF16 / BF16x2 on these
+        layer sizes) one, the unfused tcgen05 path 6 per model and one sum."""
+        import os
         if self.precision == _lib.MLP_FP32:
             return 7 * self.mlp.n_models
-        return self._tc_launches
+        fused = (self.precision in (_lib.MLP_BF16, _lib.MLP_BF16X2) and self.mlp.dims[0] % 256 == 0
+                 and max(self.mlp.dims[1:4]) <= 256 and not os.environ.get("FENNOL_MLP_UNFUSED"))
+        return 1 if fused else 6 * self.mlp.n_models + 1
 
     # --------------------------------------------------------------- launches
     def launch_forces(self, layout: BatchLayout, g: GraphBuffers, ws: Workspace, stream: int,
