@@ -852,13 +852,19 @@ class FENNIX:
             self.preprocess(**example_data)
 
     # ------------------------------------------------------------ helpers
+    def weights(self, variables=None):
+        """The species networks of ``variables`` (default: the model's) as
+        ``[model][symbol] = [(kernel, bias), ...]`` float64 arrays."""
+        variables = self.variables if variables is None else variables
+        trees = variables if isinstance(variables, (list, tuple)) else [variables]
+        return variables_to_weights(trees, self.aev_config.species_order, self.net_module.name)
+
     def _potential(self, variables) -> ANIPotential:
         key = id(variables)
         hit = self._pot_cache.get(key)
         if hit is not None and hit[0] is variables:
             return hit[1]
-        trees = variables if isinstance(variables, (list, tuple)) else [variables]
-        weights = variables_to_weights(trees, self.aev_config.species_order, self.net_module.name)
+        weights = self.weights(variables)
         pot = ANIPotential(self.aev_config, self.mlp_config, weights=weights,
                            precision=self.precision, device=self.device)
         self._pot_cache = {key: (variables, pot)}
