@@ -357,6 +357,7 @@ k_aev_forward(const float4* __restrict__ xyzs, int n, const int* __restrict__ at
               const unsigned* __restrict__ nbr_shift, const int* __restrict__ nbr_count, int cap,
               const AevConst K, const int* __restrict__ atom_row, int out_kind, void* __restrict__ out,
               void* __restrict__ out_lo, int ld, int* status) {
+  pdl_wait();
   extern __shared__ __align__(16) char smem_c[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int i = blockIdx.x * kAevWarps + warp;
@@ -468,6 +469,7 @@ k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ a
                const unsigned* __restrict__ nbr_shift, const int* __restrict__ nbr_count, int cap,
                const AevConst K, const int* __restrict__ atom_row, const float* __restrict__ daev,
                int ld, float4* __restrict__ forces, float* __restrict__ atom_virial, int* status) {
+  pdl_wait();
   extern __shared__ __align__(16) char smem_c[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int i = blockIdx.x * kAevWarps + warp;
@@ -690,6 +692,7 @@ k_aev_tangent(const float4* __restrict__ xyzs, int n, const int* __restrict__ at
               const unsigned* __restrict__ nbr_shift, const int* __restrict__ nbr_count, int cap,
               const AevConst K, const int* __restrict__ atom_row, const float4* __restrict__ du,
               float* __restrict__ out, int ld, int* status) {
+  pdl_wait();
   extern __shared__ __align__(16) char smem_c[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int i = blockIdx.x * kAevWarps + warp;
@@ -822,6 +825,7 @@ k_aev_tangent(const float4* __restrict__ xyzs, int n, const int* __restrict__ at
 
 __global__ void k_pack(const float* __restrict__ coords, const int* __restrict__ sp, int n,
                        float4* __restrict__ xyzs) {
+  pdl_wait();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   xyzs[i] = make_float4(coords[3 * i], coords[3 * i + 1], coords[3 * i + 2], __int_as_float(sp[i]));
@@ -875,7 +879,7 @@ extern "C" int fennol_pack_atoms(const float* coords, const int* species_idx, in
                                  void* stream) {
   if (natoms < 0 || (natoms > 0 && (!coords || !species_idx || !xyzs))) return FENNOL_ERR_INVALID;
   if (natoms == 0) return FENNOL_OK;
-  k_pack<<<(natoms + 255) / 256, 256, 0, (cudaStream_t)stream>>>(coords, species_idx, natoms,
+  FNL_LAUNCH_PDL(k_pack, (natoms + 255) / 256, 256, 0, (cudaStream_t)stream, coords, species_idx, natoms,
                                                                   (float4*)xyzs);
   FNL_CHECK_LAUNCH();
   return FENNOL_OK;
@@ -900,9 +904,9 @@ extern "C" int fennol_aev_forward(const float* xyzs, int natoms, const int* atom
   bool launched = dispatch(K, [&](auto ks) {
     size_t smem = set_smem((const void*)ks.fwd, (size_t)kAevWarps * stage_bytes(capacity));
     if (!smem) return false;
-    ks.fwd<<<blocks, kAevWarps * 32, smem, (cudaStream_t)stream>>>(
+    if (launch_pdl(ks.fwd, blocks, kAevWarps * 32, smem, (cudaStream_t)stream, 
         (const float4*)xyzs, natoms, atom_sys, sys_cell, nbr_j, nbr_shift, nbr_count, capacity, K,
-        atom_row, out_kind, out, out_lo, ld, status);
+        atom_row, out_kind, out, out_lo, ld, status) != cudaSuccess) return false;
     return true;
   });
   if (!launched) return FENNOL_ERR_UNSUPPORTED;
@@ -927,9 +931,9 @@ static int aev_backward_launch(const float* xyzs, int natoms, const int* atom_sy
     auto fn = atom_virial ? ks.bwdv : ks.bwd;
     size_t smem = set_smem((const void*)fn, bytes);
     if (!smem) return false;
-    fn<<<blocks, kAevWarps * 32, smem, (cudaStream_t)stream>>>(
+    if (launch_pdl(fn, blocks, kAevWarps * 32, smem, (cudaStream_t)stream, 
         (const float4*)xyzs, natoms, atom_sys, sys_cell, nbr_j, nbr_shift, nbr_count, capacity, K,
-        atom_row, daev, ld, (float4*)forces4, atom_virial, status);
+        atom_row, daev, ld, (float4*)forces4, atom_virial, status) != cudaSuccess) return false;
     return true;
   });
   if (!launched) return FENNOL_ERR_UNSUPPORTED;
@@ -973,9 +977,9 @@ extern "C" int fennol_aev_tangent(const float* xyzs, int natoms, const int* atom
   bool launched = dispatch(K, [&](auto ks) {
     size_t smem = set_smem((const void*)ks.tan, bytes);
     if (!smem) return false;
-    ks.tan<<<blocks, kAevWarps * 32, smem, (cudaStream_t)stream>>>(
+    if (launch_pdl(ks.tan, blocks, kAevWarps * 32, smem, (cudaStream_t)stream, 
         (const float4*)xyzs, natoms, atom_sys, sys_cell, nbr_j, nbr_shift, nbr_count, capacity, K,
-        atom_row, (const float4*)du4, out, ld, status);
+        atom_row, (const float4*)du4, out, ld, status) != cudaSuccess) return false;
     return true;
   });
   if (!launched) return FENNOL_ERR_UNSUPPORTED;

@@ -1,5 +1,6 @@
 // Shared device helpers for the fennol_b200 kernels (sm_100a).
 #pragma once
+#include <utility>
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 #include <stdint.h>
@@ -74,6 +75,33 @@ __host__ __device__ __forceinline__ int triu_pair(int s1, int s2, int S) {
 }
 
 }  // namespace fnl
+
+// Programmatic dependent launch: a kernel launched with launch_pdl may be
+// scheduled while the previous kernel of the stream drains; it must call
+// pdl_wait() before touching memory, which returns once that kernel has
+// completed and its writes are visible (a no-op for ordinary launches).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
+#define FNL_LAUNCH_PDL(...)                                      \
+  do {                                                           \
+    if (launch_pdl(__VA_ARGS__) != cudaSuccess) return FENNOL_ERR_CUDA; \
+  } while (0)
 
 #define FNL_CHECK_LAUNCH()                                   \
   do {                                                       \

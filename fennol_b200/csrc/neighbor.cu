@@ -70,6 +70,7 @@ __host__ size_t ws_layout(int n, int c, char* base, GraphWs* w) {
 // ---------------------------------------------------------------------------
 __global__ void k_prepare(const float* __restrict__ coords, int n, const int* __restrict__ atom_sys,
                           SysView sv, GraphWs w, const int* enable_flag) {
+  pdl_wait();
   if (enable_flag && *enable_flag == 0) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -112,6 +113,7 @@ __global__ void k_prepare(const float* __restrict__ coords, int n, const int* __
 // 2. exclusive scan of the cell histogram (one block), cursor = start.
 // ---------------------------------------------------------------------------
 __global__ void k_scan(GraphWs w, int c, const int* enable_flag) {
+  pdl_wait();
   if (enable_flag && *enable_flag == 0) return;
   __shared__ int warp_sums[32];
   __shared__ int carry;
@@ -156,6 +158,7 @@ __global__ void k_scan(GraphWs w, int c, const int* enable_flag) {
 // 3. scatter atoms into their cells (order inside a cell is arbitrary until
 //    k_sort_cells puts each cell in increasing index order).
 __global__ void k_scatter(int n, GraphWs w, const int* enable_flag) {
+  pdl_wait();
   if (enable_flag && *enable_flag == 0) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -228,6 +231,7 @@ __device__ __forceinline__ void row_finish(int i, int count, int cap, int* __res
 constexpr int kCellSortMax = 512;  // larger cells (densities far above a liquid's) keep scatter order
 
 __global__ void __launch_bounds__(256) k_sort_cells(int c, GraphWs w, const int* enable_flag) {
+  pdl_wait();
   if (enable_flag && *enable_flag == 0) return;
   __shared__ int buf[8][kCellSortMax];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -279,14 +283,11 @@ __global__ void __launch_bounds__(256) k_sort_cells(int c, GraphWs w, const int*
 //     the cell sizes; kept pairs go straight to the row in candidate order
 //     (stencil cell, then atom index), which makes the rows deterministic.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBuildWarps * 32)
-k_build_cells(int n, const int* __restrict__ atom_sys, SysView sv, GraphWs w, float rc2, int cap,
-              int* __restrict__ nbr_j, unsigned* __restrict__ nbr_shift, int* __restrict__ nbr_count,
-              int* status, const int* enable_flag) {
-  if (enable_flag && *enable_flag == 0) return;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int i = blockIdx.x * kBuildWarps + warp;
-  if (i >= n) return;
+// Row of atom i from its 27 stencil cells (warp-collective).
+__device__ __forceinline__ void cell_row(int i, const int* __restrict__ atom_sys, const SysView& sv,
+                                         const GraphWs& w, float rc2, int cap, int* __restrict__ nbr_j,
+                                         unsigned* __restrict__ nbr_shift, int* __restrict__ nbr_count,
+                                         int* status, int lane) {
   const int cell = w.atom_cell[i];
   if (cell < 0) return;  // all-pairs system
   const int b = atom_sys[i];
@@ -349,17 +350,25 @@ k_build_cells(int n, const int* __restrict__ atom_sys, SysView sv, GraphWs w, fl
   row_finish(i, count, cap, nbr_count, status, lane);
 }
 
+__global__ void __launch_bounds__(kBuildWarps * 32)
+k_build_cells(int n, const int* __restrict__ atom_sys, SysView sv, GraphWs w, float rc2, int cap,
+              int* __restrict__ nbr_j, unsigned* __restrict__ nbr_shift, int* __restrict__ nbr_count,
+              int* status, const int* enable_flag) {
+  pdl_wait();
+  if (enable_flag && *enable_flag == 0) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int i = blockIdx.x * kBuildWarps + warp; i < n; i += gridDim.x * kBuildWarps)
+    cell_row(i, atom_sys, sv, w, rc2, cap, nbr_j, nbr_shift, nbr_count, status, lane);
+}
+
+
 // ---------------------------------------------------------------------------
 // 4b. all-pairs rows (molecules, boxes too small for a 3x3x3 cell stencil).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBuildWarps * 32)
-k_build_allpairs(int n, const int* __restrict__ atom_sys, SysView sv, GraphWs w, float rc2, int cap,
-                 int* __restrict__ nbr_j, unsigned* __restrict__ nbr_shift, int* __restrict__ nbr_count,
-                 int* status, const int* enable_flag) {
-  if (enable_flag && *enable_flag == 0) return;
-  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int i = blockIdx.x * kBuildWarps + warp;
-  if (i >= n) return;
+__device__ __forceinline__ void allpairs_row(int i, const int* __restrict__ atom_sys, const SysView& sv,
+                                             const GraphWs& w, float rc2, int cap, int* __restrict__ nbr_j,
+                                             unsigned* __restrict__ nbr_shift, int* __restrict__ nbr_count,
+                                             int* status, int lane) {
   if (w.atom_cell[i] >= 0) return;  // cell-list system
   const size_t base = (size_t)i * cap;
   int b = atom_sys[i];
@@ -391,10 +400,19 @@ k_build_allpairs(int n, const int* __restrict__ atom_sys, SysView sv, GraphWs w,
   row_finish(i, count, cap, nbr_count, status, lane);
 }
 
-__global__ void k_count_rebuild(int* status, const int* enable_flag) {
+// Also counts the rebuild (one per enabled build) in the status words.
+__global__ void __launch_bounds__(kBuildWarps * 32)
+k_build_allpairs(int n, const int* __restrict__ atom_sys, SysView sv, GraphWs w, float rc2, int cap,
+                 int* __restrict__ nbr_j, unsigned* __restrict__ nbr_shift, int* __restrict__ nbr_count,
+                 int* status, const int* enable_flag) {
+  pdl_wait();
   if (enable_flag && *enable_flag == 0) return;
-  if (status) atomicAdd(status + ST_REBUILD_COUNT, 1);
+  if (status && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(status + ST_REBUILD_COUNT, 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int i = blockIdx.x * kBuildWarps + warp; i < n; i += gridDim.x * kBuildWarps)
+    allpairs_row(i, atom_sys, sv, w, rc2, cap, nbr_j, nbr_shift, nbr_count, status, lane);
 }
+
 
 // ---------------------------------------------------------------------------
 // Filter a list to a smaller cutoff (update_skin / GraphFilter).
@@ -405,6 +423,7 @@ k_filter(const float* __restrict__ coords, int n, const int* __restrict__ atom_s
          const unsigned* __restrict__ in_shift, const int* __restrict__ in_count, int in_cap,
          float rc2, int out_cap, int* __restrict__ out_j, unsigned* __restrict__ out_shift,
          int* __restrict__ out_count, int* status) {
+  pdl_wait();
   int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
   if (warp >= n) return;
@@ -522,29 +541,27 @@ extern "C" int fennol_graph_build(const float* coords, int natoms, const int* at
   }
   int tb = 256;
   int gb = (natoms + tb - 1) / tb;
-  k_prepare<<<gb, tb, 0, st>>>(coords, natoms, atom_sys, sv, w, enable_flag);
+  FNL_LAUNCH_PDL(k_prepare, gb, tb, 0, st, coords, natoms, atom_sys, sv, w, enable_flag);
   FNL_CHECK_LAUNCH();
   if (ncells_total > 0) {
-    k_scan<<<1, 1024, 0, st>>>(w, ncells_total, enable_flag);
+    FNL_LAUNCH_PDL(k_scan, 1, 1024, 0, st, w, ncells_total, enable_flag);
     FNL_CHECK_LAUNCH();
-    k_scatter<<<gb, tb, 0, st>>>(natoms, w, enable_flag);
+    FNL_LAUNCH_PDL(k_scatter, gb, tb, 0, st, natoms, w, enable_flag);
     FNL_CHECK_LAUNCH();
-    k_sort_cells<<<(ncells_total + 7) / 8, 256, 0, st>>>(ncells_total, w, enable_flag);
+    FNL_LAUNCH_PDL(k_sort_cells, (ncells_total + 7) / 8, 256, 0, st, ncells_total, w, enable_flag);
     FNL_CHECK_LAUNCH();
   }
-  int gw = (natoms + kBuildWarps - 1) / kBuildWarps;
+  // grid-stride row builders: a capped grid keeps the launch cheap when the
+  // enable flag turns the build into a no-op
+  int gw = std::min((natoms + kBuildWarps - 1) / kBuildWarps, 148 * 16);
   if (ncells_total > 0) {
-    k_build_cells<<<gw, kBuildWarps * 32, 0, st>>>(natoms, atom_sys, sv, w, rc2, capacity, nbr_j, nbr_shift,
+    FNL_LAUNCH_PDL(k_build_cells, gw, kBuildWarps * 32, 0, st, natoms, atom_sys, sv, w, rc2, capacity, nbr_j, nbr_shift,
                                                     nbr_count, status, enable_flag);
     FNL_CHECK_LAUNCH();
   }
-  k_build_allpairs<<<gw, kBuildWarps * 32, 0, st>>>(natoms, atom_sys, sv, w, rc2, capacity, nbr_j, nbr_shift,
+  FNL_LAUNCH_PDL(k_build_allpairs, gw, kBuildWarps * 32, 0, st, natoms, atom_sys, sv, w, rc2, capacity, nbr_j, nbr_shift,
                                                      nbr_count, status, enable_flag);
   FNL_CHECK_LAUNCH();
-  if (status) {
-    k_count_rebuild<<<1, 1, 0, st>>>(status, enable_flag);
-    FNL_CHECK_LAUNCH();
-  }
   return FENNOL_OK;
 }
 
@@ -560,7 +577,7 @@ extern "C" int fennol_graph_filter(const float* coords, int natoms, const int* a
   float rc2 = (float)(cutoff * cutoff);
   int threads = 256;
   long long blocks = ((long long)natoms * 32 + threads - 1) / threads;
-  k_filter<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(
+  FNL_LAUNCH_PDL(k_filter, (unsigned)blocks, threads, 0, (cudaStream_t)stream, 
       coords, natoms, atom_sys, sys_cell, in_j, in_shift, in_count, in_capacity, rc2, out_capacity,
       out_j, out_shift, out_count, status);
   FNL_CHECK_LAUNCH();

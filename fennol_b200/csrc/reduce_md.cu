@@ -23,6 +23,7 @@ __global__ void k_energy_partial(const float* __restrict__ e_rows, const int* __
                                  const int* __restrict__ sys_start, const int* __restrict__ chunk_off,
                                  int nsys, double scale, double* __restrict__ partial,
                                  double* __restrict__ e_atom) {
+  pdl_wait();
   __shared__ double part[256];
   const int total = chunk_off[nsys];
   for (int w = blockIdx.x; w < total; w += gridDim.x) {
@@ -54,6 +55,7 @@ __global__ void k_energy_partial(const float* __restrict__ e_rows, const int* __
 
 __global__ void k_energy_final(const int* __restrict__ chunk_off, int nsys, const double* __restrict__ partial,
                                double* __restrict__ energy) {
+  pdl_wait();
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= nsys) return;
   double s = 0.0;
@@ -63,6 +65,7 @@ __global__ void k_energy_final(const int* __restrict__ chunk_off, int nsys, cons
 
 // chunk_off[b] = sum_{b' < b} max(1, ceil(n_b' / kRedChunk)) (one block, tiled scan).
 __global__ void k_chunk_offsets(const int* __restrict__ sys_start, int nsys, int* __restrict__ chunk_off) {
+  pdl_wait();
   __shared__ int warp_sums[32];
   __shared__ int carry;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -104,6 +107,7 @@ __global__ void k_chunk_offsets(const int* __restrict__ sys_start, int nsys, int
 }
 
 __global__ void k_forces_finalize(const float4* __restrict__ f4, int n, float scale, float* __restrict__ f) {
+  pdl_wait();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   float4 v = f4[i];
@@ -203,6 +207,7 @@ __global__ void k_md_step(int n, double dt, double* __restrict__ x, double* __re
                           float* __restrict__ coords,
                           const int* __restrict__ sp, float4* __restrict__ xyzs,
                           const double* __restrict__ x_ref, double half_skin2, int* rebuild_flag) {
+  pdl_wait();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   unsigned long long step = a2 ? *step_counter : 0ull;
@@ -222,6 +227,7 @@ __global__ void k_md_step_systems(int n, double dt, double* __restrict__ x, doub
                                   const unsigned long long* __restrict__ sys_step, float* __restrict__ coords,
                                   const int* __restrict__ sp, float4* __restrict__ xyzs,
                                   const double* __restrict__ x_ref, double half_skin2, int* rebuild_flag) {
+  pdl_wait();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int b = atom_sys[i];
@@ -232,21 +238,26 @@ __global__ void k_md_step_systems(int n, double dt, double* __restrict__ x, doub
 }
 
 __global__ void k_inc_steps(int nsys, unsigned long long* __restrict__ sys_step) {
+  pdl_wait();
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b < nsys) sys_step[b] += 1ull;
 }
 
-__global__ void k_inc_counter(unsigned long long* c) { *c += 1ull; }
+__global__ void k_inc_counter(unsigned long long* c) {
+  pdl_wait(); *c += 1ull; }
 
 __global__ void k_mark_rebuilt(int n, const double* __restrict__ x, double* __restrict__ x_ref, int* flag) {
+  pdl_wait();
   if (*flag == 0) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < 3 * n) x_ref[i] = x[i];
 }
-__global__ void k_clear_flag(int* flag) { *flag = 0; }
+__global__ void k_clear_flag(int* flag) {
+  pdl_wait(); *flag = 0; }
 
 __global__ void k_kinetic(int n, const double* __restrict__ v, const double* __restrict__ inv_mass,
                           double* out) {
+  pdl_wait();
   __shared__ double part[1024];
   double s = 0.0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -274,6 +285,7 @@ extern "C" size_t fennol_energy_workspace_bytes(int natoms, int nsys) {
 __global__ void __launch_bounds__(256) k_virial_reduce(const float* __restrict__ av,
                                                        const int* __restrict__ sys_start, double scale,
                                                        double* __restrict__ vir) {
+  pdl_wait();
   __shared__ double red[9][256];
   const int b = blockIdx.x, tid = threadIdx.x;
   double acc[9];
@@ -299,7 +311,7 @@ extern "C" int fennol_virial_reduce(const float* atom_virial, int natoms, const 
   if (natoms < 0 || nsys < 0) return FENNOL_ERR_INVALID;
   if (nsys == 0) return FENNOL_OK;
   if (!sys_start || !virial || (natoms > 0 && !atom_virial)) return FENNOL_ERR_INVALID;
-  k_virial_reduce<<<nsys, 256, 0, (cudaStream_t)stream>>>(atom_virial, sys_start, scale, virial);
+  FNL_LAUNCH_PDL(k_virial_reduce, nsys, 256, 0, (cudaStream_t)stream, atom_virial, sys_start, scale, virial);
   FNL_CHECK_LAUNCH();
   return FENNOL_OK;
 }
@@ -315,14 +327,14 @@ extern "C" int fennol_energy_reduce(const float* e_rows, const int* atom_row, in
   cudaStream_t st = (cudaStream_t)stream;
   int* chunk_off = (int*)workspace;
   double* partial = (double*)((char*)workspace + ((sizeof(int) * (size_t)(nsys + 1) + 255) / 256 * 256));
-  k_chunk_offsets<<<1, 1024, 0, st>>>(sys_start, nsys, chunk_off);
+  FNL_LAUNCH_PDL(k_chunk_offsets, 1, 1024, 0, st, sys_start, nsys, chunk_off);
   FNL_CHECK_LAUNCH();
   int blocks = natoms / kRedChunk + nsys;
   if (blocks > 4 * 148) blocks = 4 * 148;
-  k_energy_partial<<<blocks, 256, 0, st>>>(e_rows, atom_row, sys_start, chunk_off, nsys, scale, partial,
+  FNL_LAUNCH_PDL(k_energy_partial, blocks, 256, 0, st, e_rows, atom_row, sys_start, chunk_off, nsys, scale, partial,
                                            e_atom);
   FNL_CHECK_LAUNCH();
-  k_energy_final<<<(nsys + 127) / 128, 128, 0, st>>>(chunk_off, nsys, partial, energy);
+  FNL_LAUNCH_PDL(k_energy_final, (nsys + 127) / 128, 128, 0, st, chunk_off, nsys, partial, energy);
   FNL_CHECK_LAUNCH();
   return FENNOL_OK;
 }
@@ -332,7 +344,7 @@ extern "C" int fennol_forces_finalize(const float* forces4, int natoms, float sc
   if (natoms < 0) return FENNOL_ERR_INVALID;
   if (natoms == 0) return FENNOL_OK;
   if (!forces4 || !forces) return FENNOL_ERR_INVALID;
-  k_forces_finalize<<<(natoms + 255) / 256, 256, 0, (cudaStream_t)stream>>>((const float4*)forces4, natoms,
+  FNL_LAUNCH_PDL(k_forces_finalize, (natoms + 255) / 256, 256, 0, (cudaStream_t)stream, (const float4*)forces4, natoms,
                                                                              scale, forces);
   FNL_CHECK_LAUNCH();
   return FENNOL_OK;
@@ -350,12 +362,12 @@ extern "C" int fennol_md_step(int natoms, double dt, double* x, double* v, const
   if (!x || !v || !inv_mass || !forces4) return FENNOL_ERR_INVALID;
   if (xyzs && !species_idx) return FENNOL_ERR_INVALID;
   cudaStream_t st = (cudaStream_t)stream;
-  k_md_step<<<(natoms + 255) / 256, 256, 0, st>>>(
+  FNL_LAUNCH_PDL(k_md_step, (natoms + 255) / 256, 256, 0, st, 
       natoms, dt, x, v, inv_mass, (const float4*)forces4, force_scale, a1, a2, seed, step_counter,
       coords, species_idx, (float4*)xyzs, x_ref, half_skin * half_skin, rebuild_flag);
   FNL_CHECK_LAUNCH();
   if (step_counter) {
-    k_inc_counter<<<1, 1, 0, st>>>(step_counter);
+    FNL_LAUNCH_PDL(k_inc_counter, 1, 1, 0, st, step_counter);
     FNL_CHECK_LAUNCH();
   }
   return FENNOL_OK;
@@ -374,11 +386,11 @@ extern "C" int fennol_md_step_systems(int natoms, int nsys, double dt, double* x
     return FENNOL_ERR_INVALID;
   if (xyzs && !species_idx) return FENNOL_ERR_INVALID;
   cudaStream_t st = (cudaStream_t)stream;
-  k_md_step_systems<<<(natoms + 255) / 256, 256, 0, st>>>(
+  FNL_LAUNCH_PDL(k_md_step_systems, (natoms + 255) / 256, 256, 0, st, 
       natoms, dt, x, v, inv_mass, (const float4*)forces4, force_scale, a1, a2, atom_sys, sys_start, sys_seed,
       sys_step, coords, species_idx, (float4*)xyzs, x_ref, half_skin * half_skin, rebuild_flag);
   FNL_CHECK_LAUNCH();
-  k_inc_steps<<<(nsys + 255) / 256, 256, 0, st>>>(nsys, sys_step);
+  FNL_LAUNCH_PDL(k_inc_steps, (nsys + 255) / 256, 256, 0, st, nsys, sys_step);
   FNL_CHECK_LAUNCH();
   return FENNOL_OK;
 }
@@ -388,10 +400,10 @@ extern "C" int fennol_md_mark_rebuilt(int natoms, const double* x, double* x_ref
   if (natoms < 0 || !x || !x_ref || !rebuild_flag) return FENNOL_ERR_INVALID;
   cudaStream_t st = (cudaStream_t)stream;
   if (natoms > 0) {
-    k_mark_rebuilt<<<(3 * natoms + 255) / 256, 256, 0, st>>>(natoms, x, x_ref, rebuild_flag);
+    FNL_LAUNCH_PDL(k_mark_rebuilt, (3 * natoms + 255) / 256, 256, 0, st, natoms, x, x_ref, rebuild_flag);
     FNL_CHECK_LAUNCH();
   }
-  k_clear_flag<<<1, 1, 0, st>>>(rebuild_flag);
+  FNL_LAUNCH_PDL(k_clear_flag, 1, 1, 0, st, rebuild_flag);
   FNL_CHECK_LAUNCH();
   return FENNOL_OK;
 }
@@ -400,7 +412,7 @@ extern "C" int fennol_md_kinetic(int natoms, const double* v, const double* inv_
                                  void* stream) {
   if (natoms < 0 || !kinetic) return FENNOL_ERR_INVALID;
   if (natoms > 0 && (!v || !inv_mass)) return FENNOL_ERR_INVALID;
-  k_kinetic<<<1, 1024, 0, (cudaStream_t)stream>>>(natoms, v, inv_mass, kinetic);
+  FNL_LAUNCH_PDL(k_kinetic, 1, 1024, 0, (cudaStream_t)stream, natoms, v, inv_mass, kinetic);
   FNL_CHECK_LAUNCH();
   return FENNOL_OK;
 }

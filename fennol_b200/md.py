@@ -161,8 +161,8 @@ class MDEngine:
         included; they return at once when no rebuild is due)."""
         n = 2  # md step + counter
         if self.trigger == "displacement":
-            # prepare/scan/scatter/sort cells/cells/allpairs/count + mark/clear
-            n += (7 if self.graph_buf.ncells > 0 else 3) + 2
+            # prepare/scan/scatter/sort cells/cells/allpairs + mark/clear
+            n += (6 if self.graph_buf.ncells > 0 else 2) + 2
         n += 1 if self.skin > 0 else 0
         n += 1 + self.pot.mlp_launches() + 3 + 1  # aev fwd, mlp, energy sum (3), aev bwd
         return n
