@@ -37,7 +37,6 @@ Every compute step runs in ``libfennol_b200.so``; there is no CPU path.
 from __future__ import annotations
 
 import dataclasses
-import math
 import re
 from collections import OrderedDict
 from copy import deepcopy

@@ -30,7 +30,7 @@ import torch
 from . import _lib
 from ._lib import call
 from .params import atomic_masses
-from .potential import ANIPotential, C_ptr, GraphBuffers, HARTREE_TO_KCALMOL, Workspace, _ptr
+from .potential import ANIPotential, GraphBuffers, HARTREE_TO_KCALMOL, _ptr
 
 # atomic-unit constants of src/fennol/utils/atomic_units.py
 _MPROT = 1836.1526734252586

@@ -11,7 +11,6 @@ force adjoint once.
 
 import argparse
 
-import numpy as np
 import torch
 
 from .potential import ANIPotential
