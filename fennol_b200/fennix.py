@@ -50,7 +50,7 @@ from ._lib import call
 from .fnx import load_model_dict, save_model_dict
 from .params import (PERIODIC_TABLE, PERIODIC_TABLE_REV_IDX, AEVConfig, MLPConfig,
                      init_weights, variables_to_weights, weights_to_variables)
-from .potential import (MAX_ROW, ANIPotential, BatchLayout, Workspace, _ceil, _ptr, _stream)
+from .potential import MAX_ROW, ANIPotential, BatchLayout, Workspace, _ceil, _stream
 
 # multipliers from Hartree (atomic units, fennol/utils/atomic_units.py)
 ENERGY_UNITS = {
