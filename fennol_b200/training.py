@@ -95,7 +95,7 @@ class LossGradient:
     """
 
     def __init__(self, pot: ANIPotential, w_e: float = 1.0, w_f: float = 10.0,
-                 dtype: torch.dtype = torch.float32):
+                 dtype: torch.dtype = torch.float32, use_graphs: bool = True):
         if pot.mlp.n_models != 1:
             raise ValueError("training gradients are computed for one model")
         self.pot, self.w_e, self.w_f, self.dtype = pot, w_e, w_f, dtype
@@ -103,28 +103,33 @@ class LossGradient:
         self.layers = {sym: [(torch.tensor(w, dtype=dtype, device=dev), torch.tensor(b, dtype=dtype, device=dev))
                              for w, b in layers]
                        for sym, layers in pot.weights[0].items()}
+        self.shapes = [tuple(t_.shape) for sym in pot.aev_cfg.species_order for wb in self.layers[sym]
+                       for t_ in wb]
+        self.use_graphs = use_graphs
+        self._rec = None      # captured pass of the current batch
+        self._seen = None     # batch key of the previous call
 
-    def __call__(self, coordinates, species, natoms, e_ref, f_ref, cells=None):
+    # ------------------------------------------------------------ device pass
+    def _device_pass(self, layout, g, ws, coords, e_ref, f_ref, out):
+        """Every launch of one loss + gradient evaluation, from device inputs
+        to the flat device output [status words, E loss, F loss, gradient].
+        No host synchronisation, so it can be captured in a CUDA graph."""
         pot, dev = self.pot, self.pot.device
-        natoms = np.asarray(natoms).reshape(-1)
-        energy, forces = pot.energy_and_forces(coordinates, species, natoms, cells)
-        layout, g, ws = next(iter(pot._cache.values()))
-        B, N = int(natoms.shape[0]), int(layout.n)
-        e_ref_t = torch.as_tensor(np.asarray(e_ref, np.float64), device=dev)
-        f_ref_t = torch.as_tensor(np.asarray(f_ref, np.float64), device=dev).reshape(N, 3)
-        de = energy - e_ref_t
-        df = forces.double() - f_ref_t
-        losses = torch.stack([(de ** 2).mean(), (df ** 2).mean()])
+        st = _stream(dev)
+        B, N = layout.nsys, layout.n
+        pot._launch_all(layout, g, ws, coords, st, True)
+        energy, forces = ws.energy, ws.forces[:N]
+        de = energy - e_ref
+        df = forces.double() - f_ref
         c_sys = (2.0 * self.w_e / B) * de                      # dL/dE_b
         u = (2.0 * self.w_f / (3 * N)) * df                    # dL/dF
         du4 = torch.zeros((N, 4), dtype=torch.float32, device=dev)
         du4[:, :3] = u.float()
         d0 = ws.x.shape[1]
         t = torch.zeros((layout.rows, d0), dtype=torch.float32, device=dev)
-        status = torch.zeros(_lib.STATUS_WORDS, dtype=torch.int32, device=dev)
         call("fennol_aev_tangent", ws.xyzs.data_ptr(), N, layout.t_atom_sys.data_ptr(), layout.t_cell.data_ptr(),
              g.rad_j.data_ptr(), g.rad_s.data_ptr(), g.rad_n.data_ptr(), g.cap_r, C_ptr(pot.params),
-             layout.t_atom_row.data_ptr(), du4.data_ptr(), t.data_ptr(), d0, status.data_ptr(), _stream(dev))
+             layout.t_atom_row.data_ptr(), du4.data_ptr(), t.data_ptr(), d0, ws.status.data_ptr(), st)
         F = pot.aev_cfg.aev_length
         x = ws.x.float()
         if ws.x_lo is not None:
@@ -138,35 +143,88 @@ class LossGradient:
             sl = slice(row0, row0 + count)
             dev_grads[sym] = network_loss_gradient(x[sl, :F].to(self.dtype), t[sl, :F].to(self.dtype),
                                                    c_row[sl], self.layers[sym], pot.mlp_cfg.celu_alpha)
-        # one transfer for the whole gradient
-        parts, shapes = [], []
+        out_small, out_grad = out
+        torch.cat([ws.status.double(), torch.stack([self.w_e * (de ** 2).mean(), self.w_f * (df ** 2).mean()])],
+                  out=out_small)
+        parts = []
         for sym in pot.aev_cfg.species_order:
             for l, (W, b) in enumerate(self.layers[sym]):
-                if sym in dev_grads:
-                    gW, gb = dev_grads[sym][l]
-                else:
-                    gW, gb = torch.zeros_like(W), torch.zeros_like(b)
+                gW, gb = dev_grads[sym][l] if sym in dev_grads else (torch.zeros_like(W), torch.zeros_like(b))
                 parts += [gW.reshape(-1), gb.reshape(-1)]
-                shapes += [tuple(W.shape), tuple(b.shape)]
-        flat = torch.cat([p_.double() for p_ in parts]).cpu().numpy()
+        torch.cat(parts, out=out_grad)
+
+    def __call__(self, coordinates, species, natoms, e_ref, f_ref, cells=None):
+        pot, dev = self.pot, self.pot.device
+        natoms = np.asarray(natoms).reshape(-1)
+        species = np.asarray(species)
+        key = (species.tobytes(), natoms.tobytes(),
+               None if cells is None else np.asarray(cells, np.float32).tobytes())
+        coords = torch.as_tensor(coordinates, dtype=torch.float32).to(dev).reshape(-1, 3).contiguous()
+        e_ref_t = torch.as_tensor(np.asarray(e_ref, np.float64), device=dev).reshape(-1)
+        f_ref_t = torch.as_tensor(np.asarray(f_ref, np.float64), device=dev).reshape(-1, 3)
+        rec = self._rec if (self.use_graphs and self._rec is not None and self._rec["key"] == key) else None
+        if rec is not None:
+            rec["coords"].copy_(coords)
+            rec["e_ref"].copy_(e_ref_t)
+            rec["f_ref"].copy_(f_ref_t)
+            rec["graph"].replay()
+            small = rec["out"][0].cpu().numpy()
+            if not self._overflowed(small):
+                return self._unpack(small, rec["out"][1], rec["layout"], rec["ws"])
+            self._rec = None  # lists too short for these positions: rebuild eagerly
+        # eager pass: sizes the lists (regrowing on overflow) and checks them
+        pot.energy_and_forces(coords, species, natoms, cells)
+        layout, g, ws = next(iter(pot._cache.values()))
+        out = self._outputs()
+        self._device_pass(layout, g, ws, coords, e_ref_t, f_ref_t, out)
+        small = out[0].cpu().numpy()
+        if self._overflowed(small):
+            raise RuntimeError("neighbour or angular capacity exceeded during the gradient pass")
+        result = self._unpack(small, out[1], layout, ws)
+        if self.use_graphs and self._seen == key:
+            self._capture(key, layout, g, ws, coords, e_ref_t, f_ref_t)
+        self._seen = key
+        return result
+
+    def _outputs(self):
+        """(status words + the two loss terms in float64, flat gradient in the sweep's dtype)."""
+        dev = self.pot.device
+        return (torch.empty(_lib.STATUS_WORDS + 2, dtype=torch.float64, device=dev),
+                torch.empty(sum(int(np.prod(s_)) for s_ in self.shapes), dtype=self.dtype, device=dev))
+
+    def _capture(self, key, layout, g, ws, coords, e_ref, f_ref):
+        rec = {"key": key, "layout": layout, "ws": ws, "coords": coords.clone(), "e_ref": e_ref.clone(),
+               "f_ref": f_ref.clone(), "out": self._outputs()}
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            self._device_pass(layout, g, ws, rec["coords"], rec["e_ref"], rec["f_ref"], rec["out"])
+        rec["graph"] = graph
+        self._rec = rec
+
+    @staticmethod
+    def _overflowed(host: np.ndarray) -> bool:
+        st = host[:_lib.STATUS_WORDS]
+        return bool(st[_lib.ST_NBR_OVERFLOW] or st[_lib.ST_FILTER_OVERFLOW] or st[_lib.ST_ANG_OVERFLOW])
+
+    def _unpack(self, small: np.ndarray, grad_dev: torch.Tensor, layout, ws):
+        """Loss terms and the gradient as views into one host copy of the flat
+        device gradient (float64 arrays for float64 sweeps, else float32)."""
+        l_e, l_f = float(small[_lib.STATUS_WORDS]), float(small[_lib.STATUS_WORDS + 1])
+        host = grad_dev.cpu().numpy()
         grads: Dict[str, List[Tuple[np.ndarray, np.ndarray]]] = {}
         pos, i = 0, 0
-        for sym in pot.aev_cfg.species_order:
+        for sym in self.pot.aev_cfg.species_order:
             layers = []
             for _ in self.layers[sym]:
                 arrs = []
                 for _k in range(2):
-                    size = int(np.prod(shapes[i]))
-                    arrs.append(flat[pos:pos + size].reshape(shapes[i]))
+                    size = int(np.prod(self.shapes[i]))
+                    arrs.append(host[pos:pos + size].reshape(self.shapes[i]))
                     pos += size
                     i += 1
                 layers.append(tuple(arrs))
             grads[sym] = layers
-        l_e, l_f = (float(v) for v in (losses * torch.tensor([self.w_e, self.w_f], dtype=losses.dtype,
-                                                              device=dev)).cpu())
-        if int(status[_lib.ST_ANG_OVERFLOW]):
-            raise RuntimeError(f"more than {_lib.MAX_ANGULAR_NEIGHBORS} angular neighbours around one atom")
-        terms = LossTerms(l_e + l_f, l_e, l_f, energy.cpu().numpy(), forces.cpu().numpy())
+        terms = LossTerms(l_e + l_f, l_e, l_f, ws.energy.cpu().numpy(), ws.forces[:layout.n].cpu().numpy())
         return terms, grads
 
 

@@ -98,3 +98,23 @@ def test_gradient_entries_match_finite_differences(cuda_device):
             fd = (lp - lm) / (2 * h)
             got = g["H"][layer][which][idx]
             assert abs(fd - got) <= 1e-3 * abs(fd) + 1e-9, (layer, which, fd, got)
+
+
+def test_replayed_gradient_equals_direct(cuda_device):
+    """From the third call on one batch the pass is one CUDA-graph replay;
+    its results must equal the direct evaluation at new positions."""
+    xyz, sp, nat = batch(16, seed=47)
+    W = init_weights(CFG, MCFG, seed=10, bias_std=0.05)
+    e_ref, f_ref = teacher_targets(xyz, sp, nat)
+    pot = ANIPotential(precision="fp32", device=cuda_device, weights=W)
+    lg = LossGradient(pot)
+    rng = np.random.default_rng(3)
+    for k in range(4):
+        x = xyz + rng.normal(scale=0.02, size=xyz.shape)
+        terms, g = lg(x, sp, nat, e_ref, f_ref)
+        ref_pot = ANIPotential(precision="fp32", device=cuda_device, weights=W, use_graphs=False)
+        t2, g2 = LossGradient(ref_pot, use_graphs=False)(x, sp, nat, e_ref, f_ref)
+        assert abs(terms.loss - t2.loss) <= 1e-6 * t2.loss, k
+        a, b = flatten(g, CFG.species_order), flatten(g2, CFG.species_order)
+        assert np.linalg.norm(a - b) <= 1e-5 * np.linalg.norm(b), k
+    assert lg._rec is not None  # the later calls replayed the captured pass
