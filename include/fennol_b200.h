@@ -93,7 +93,9 @@ size_t fennol_graph_workspace_bytes(int natoms, int ncells_total);
  * with (float)(cutoff*cutoff) (cutoff is passed in double precision so the
  * threshold rounds exactly like the reference's Python float).  General PBC wraps atoms with -floor(x @ recip)
  * first and stores shift = image + at_shift[j] - at_shift[i] (:340-346).
- * Rows are sorted by (j, shift), so the result is deterministic.
+ * A row lists its pairs in a fixed order (cell-list systems: stencil cell,
+ * then increasing j; all-pairs systems: image, then increasing j), so the
+ * result is deterministic and independent of the other systems in the batch.
  * Outputs: nbr_j[natoms*capacity], nbr_shift[natoms*capacity] (packed
  * signed bytes x | y<<8 | z<<16), nbr_count[natoms] (clamped to capacity).
  * Overflow sets status[FENNOL_ST_NBR_OVERFLOW] and the needed row length goes
