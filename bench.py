@@ -553,6 +553,16 @@ def main():
            "clocks": clocks.summary(),
            "gpu_launches": eng.launches_per_step() * args.steps,
            "rebuilds_in_run": eng.rebuild_count()}
+    # end-to-end public-API calls on every rank; the job rate uses the slowest rank
+    e2e_res = e2e(pot, box, max(5, args.steps // 3), 3)
+    if world > 1:
+        from fennol_b200.replicas import max_over_ranks
+        ms_e2e = max_over_ranks(e2e_res["ms_per_step"], device)
+        e2e_res.update(value=world * box.natoms / (ms_e2e * 1e-3), ms_per_step=ms_e2e,
+                       h2d_bytes_per_step=world * e2e_res["h2d_bytes_per_step"],
+                       d2h_bytes_per_step=world * e2e_res["d2h_bytes_per_step"])
+    # the comparisons below are single-GPU measurements, made at N = 1 only
+    extras = world == 1
     if rank == 0:
         hbm, tf_burst, tf_sust, src = measured_peaks()
         kt, mean_nbr = kernel_times(pot, eng)
@@ -591,7 +601,7 @@ def main():
                            "ms_per_launch": kd["ms_per_launch"],
                            "algorithmic_per_launch": kd.get("algorithmic_bytes_per_launch",
                                                             kd.get("algorithmic_flop_per_launch"))}
-        if precision != "fp32":
+        if precision != "fp32" and extras:
             _, pot32, eng32 = make_engine(args.workload, "fp32", device, seed=rank)
             ms32 = time_steps(eng32, max(5, args.steps // 3), 3, flush)
             v32 = box.natoms / (float(ms32.mean()) * 1e-3)
@@ -599,26 +609,27 @@ def main():
                                 "mlp_ms_per_launch": time_mlp(pot32, eng32, 10)}
             res["speedup_vs_fp32_form"] = value / world / v32
             del eng32, pot32
-        from fennol_b200.potential import ANIPotential
-        spec = ANIPotential(precision=precision, device=device, seed=0, n_models=w["n_models"],
-                            bf16_weights=True)
-        res["accuracy_vs_fp64_oracle"] = accuracy(spec, box)
-        res["accuracy_vs_fp64_oracle"]["model"] = ("unscaled N(0, 1/fan_in) random-init weights "
-                                                   "rounded to BF16 (same weights in the oracle)")
-        del spec
-        res["e2e"] = e2e(pot, box, max(5, args.steps // 3), 3)
-        if not args.skip_serving:
+        if extras:
+            from fennol_b200.potential import ANIPotential
+            spec = ANIPotential(precision=precision, device=device, seed=0, n_models=w["n_models"],
+                                bf16_weights=True)
+            res["accuracy_vs_fp64_oracle"] = accuracy(spec, box)
+            res["accuracy_vs_fp64_oracle"]["model"] = ("unscaled N(0, 1/fan_in) random-init weights "
+                                                       "rounded to BF16 (same weights in the oracle)")
+            del spec
+        res["e2e"] = e2e_res
+        if not args.skip_serving and extras:
             res["serving"] = serving_run(device)
-        if not args.skip_training:
+        if not args.skip_training and extras:
             res["training_256mol"] = training_256(device)
-        if not args.skip_98k and args.workload != "water98k":
+        if not args.skip_98k and args.workload != "water98k" and extras:
             # last: the 98k-atom engines hold several GB that later parts would work around
             del eng, pot
             torch.cuda.empty_cache()
             res["ensemble_98k"] = ensemble_98k(device, 5, 3, flush)
-        if args.nve_drift_steps > 0:
+        if args.nve_drift_steps > 0 and extras:
             res["nve_drift"] = nve_drift(device, args.nve_drift_steps)
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and extras:
             res["cpu_baseline"] = cpu_baseline(box, w["n_models"])
         print(json.dumps(res), flush=True)
     if world > 1:
