@@ -6,9 +6,9 @@
 // model of the ensemble, runs the six GEMMs of the layer chain
 //     L1 X.W1  L2 H1.W2  L3 H2.W3 (+ energy head)  B3 G3.W3^T  B2 G2.W2^T  B1 G1.W1^T
 // keeping the activations on chip:
-//   * warp 0 (one thread) streams the AEV tile and W1^T through a 2-stage TMA
-//     ring that aliases the activation buffer, and all other weights through a
-//     2-stage TMA ring;
+//   * warp 0 (one thread) streams the AEV tile and W1^T through a 3-stage TMA
+//     ring that aliases the activation buffer and the weight ring, then all
+//     other weights through the 2-stage weight ring;
 //   * warp 1 owns the 512 TMEM columns (two 256-column FP32 accumulators used
 //     alternately) and one thread issues tcgen05.mma / tcgen05.commit;
 //   * warps 2-9 are the epilogue: they read an accumulator (tcgen05.ld, one
@@ -41,7 +41,10 @@ constexpr uint32_t kActBytes = 2 * kActHalf;      // 128 KB
 constexpr int kWStages = 2;
 constexpr uint32_t kWStage = 256 * BK * 2;        // 32 KB
 constexpr uint32_t kXStage = kActBytes / 2;       // 64 KB: A hi | A lo | B (<= 256 rows)
-constexpr uint32_t kXpose = 8 * 32 * 32 * 4;      // per-epilogue-warp 32x32 transpose tiles: 32 KB
+// L1 ring: stages 0-1 alias the activation buffer, stage 2 the weight ring
+// (idle while L1 streams); stage s starts at act + s * kXStage
+constexpr int kXStages = 3;
+constexpr uint32_t kXpose = 8 * 32 * 32 * 4;      // per-epilogue-warp 32x32 dX staging tiles: 32 KB
 constexpr uint32_t kSmemMain = kActBytes + kWStages * kWStage + kXpose;  // 224 KB
 constexpr uint64_t kTimeoutNs = 2000000000ull;
 
@@ -65,10 +68,11 @@ struct FusedParams {
 
 struct Maps {
   CUtensorMap x, xlo, w1t, w2t, w3t, w3, w2, w1;
+  CUtensorMap dx;  // FP32 [rows][d0], 32 x 32 boxes, 128-byte swizzle
 };
 
 struct Bars {
-  uint64_t x_full[2], x_empty[2], w_full[kWStages], w_empty[kWStages];
+  uint64_t x_full[kXStages], x_empty[kXStages], w_full[kWStages], w_empty[kWStages];
   uint64_t acc_full[2], acc_free[2], act_ready, act_free, done, ex_ready, ex_free;
   uint32_t tmem_slot;
   int abort_flag;
@@ -110,11 +114,13 @@ __device__ __forceinline__ void act_store(uint8_t* act, int r, int n, const floa
   uint32_t h[16], l[16];
 #pragma unroll
   for (int k = 0; k < 16; ++k) {
-    __nv_bfloat16 a = __float2bfloat16_rn(v[2 * k]), b = __float2bfloat16_rn(v[2 * k + 1]);
-    h[k] = (uint32_t)__bfloat16_as_ushort(a) | ((uint32_t)__bfloat16_as_ushort(b) << 16);
-    __nv_bfloat16 c = __float2bfloat16_rn(v[2 * k] - __bfloat162float(a));
-    __nv_bfloat16 d = __float2bfloat16_rn(v[2 * k + 1] - __bfloat162float(b));
-    l[k] = (uint32_t)__bfloat16_as_ushort(c) | ((uint32_t)__bfloat16_as_ushort(d) << 16);
+    // one paired conversion per two columns for the high parts and one for the
+    // residuals (round to nearest each, as two single conversions would)
+    const __nv_bfloat162 hb = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]);
+    const float2 hf = __bfloat1622float2(hb);
+    const __nv_bfloat162 lb = __floats2bfloat162_rn(v[2 * k] - hf.x, v[2 * k + 1] - hf.y);
+    h[k] = *reinterpret_cast<const uint32_t*>(&hb);
+    l[k] = *reinterpret_cast<const uint32_t*>(&lb);
   }
   const int atom = n >> 6;
   const int j0 = (n & 63) >> 3;
@@ -141,9 +147,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
   const int M = p.n_models;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < 2; ++s) {
+    for (int s = 0; s < kXStages; ++s) {
       mbar_init(&bars->x_full[s], 1);
       mbar_init(&bars->x_empty[s], 1);
+    }
+    for (int s = 0; s < 2; ++s) {
       mbar_init(&bars->acc_full[s], 1);
       mbar_init(&bars->acc_free[s], kEpiThreads / 32);
     }
@@ -180,8 +188,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
           const int g = m * p.n_species + sp;
           if (item > 0 && !(ok = wait_bar(&bars->act_free, (item - 1) & 1, abort_flag, p.err))) break;
           for (int kc = 0; kc < p.d0 / BK; ++kc, ++xq) {
-            const int s = xq & 1;
-            const uint32_t u = xq >> 1;
+            const int s = xq % kXStages;
+            const uint32_t u = xq / kXStages;
             if (u > 0 && !(ok = wait_bar(&bars->x_empty[s], (u - 1) & 1, abort_flag, p.err))) break;
             uint8_t* st = act + s * kXStage;
             mbar_expect_tx(&bars->x_full[s], x_tx);
@@ -190,6 +198,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
             tma_load_2d(&maps.w1t, &bars->x_full[s], st + 2 * kAtom, kc * BK, g * p.d1);
           }
           if (!ok) break;
+          // the weight ring is L1 stage 2: its last chunk of this item must have
+          // been consumed (d0 / BK >= 3, so the item used stage 2)
+          {
+            const uint32_t last = xq - 1 - ((xq - 1 - 2) % kXStages);
+            if (!(ok = wait_bar(&bars->x_empty[2], (last / kXStages) & 1, abort_flag, p.err))) break;
+          }
           // weight chunks of the remaining GEMMs, in MMA order
           const CUtensorMap* wm[5] = {&maps.w2t, &maps.w3t, &maps.w3, &maps.w2, &maps.w1};
           const int rows_g[5] = {p.d2, p.d3, p.d2, p.d1, p.d0};
@@ -212,9 +226,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
       // Before the CTA can exit, every issued TMA load must have landed (on an
       // abort some stages may never be consumed).  Bounded, ignores the abort flag.
       int dummy = 0;
-      for (uint32_t s = 0; s < 2 && s < xq; ++s) {
-        const uint32_t last = xq - 1 - ((xq - 1 - s) % 2);
-        wait_bar(&bars->x_full[s], (last >> 1) & 1, &dummy, p.err);
+      for (uint32_t s = 0; s < (uint32_t)kXStages && s < xq; ++s) {
+        const uint32_t last = xq - 1 - ((xq - 1 - s) % kXStages);
+        wait_bar(&bars->x_full[s], (last / kXStages) & 1, &dummy, p.err);
       }
       for (uint32_t s = 0; s < (uint32_t)kWStages && s < wq; ++s) {
         const uint32_t last = wq - 1 - ((wq - 1 - s) % kWStages);
@@ -261,8 +275,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
             const uint32_t idesc = idesc_bf16_f32(p.d1);
             const uint32_t d = tmem + b * 256;
             for (int kc = 0; kc < p.d0 / BK; ++kc, ++xq) {
-              const int s = xq & 1;
-              if (!(ok = wait_bar(&bars->x_full[s], (xq >> 1) & 1, abort_flag, p.err))) break;
+              const int s = xq % kXStages;
+              if (!(ok = wait_bar(&bars->x_full[s], (xq / kXStages) & 1, abort_flag, p.err))) break;
               fence_after_sync();
               const uint32_t st = smem_u32(act + s * kXStage);
 #pragma unroll
@@ -342,6 +356,47 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
       fence_proxy_async();
       mbar_arrive(&bars->act_ready);
     };
+    // H = celu(Z + bias) -> act for columns [0, n); celu'(z) -> dc columns
+    // [dc0, dc0 + n).  The bias loads are issued before the TMEM load so that
+    // their latencies overlap.
+    auto celu_layer = [&](uint32_t b, const float* bias, int n, int dc0) {
+      for (int cc = half; cc < n / 32; cc += 2) {
+        float4 bb[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) bb[k] = __ldg(reinterpret_cast<const float4*>(bias + cc * 32) + k);
+        float v[32];
+        tmem_ld32(tmem + b * 256 + lane_base + cc * 32, v);
+        float* dco = dc + (size_t)(dc0 + cc * 32) * BM;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const float zz[4] = {v[4 * k] + bb[k].x, v[4 * k + 1] + bb[k].y, v[4 * k + 2] + bb[k].z,
+                               v[4 * k + 3] + bb[k].w};
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            float dh;
+            celu_pair(zz[u], p.alpha, inv_alpha, v[4 * k + u], dh);
+            dco[(size_t)(4 * k + u) * BM] = dh;  // column-major: the warp writes 128 contiguous bytes
+          }
+        }
+        act_store(act, r, cc * 32, v, with_lo);
+      }
+    };
+    // G = D * celu'(z) -> act for columns [0, n), celu' read back from dc
+    // columns [dc0, dc0 + n) (written by this thread); loads issued before the
+    // TMEM load.
+    auto mask_layer = [&](uint32_t b, int n, int dc0) {
+      for (int cc = half; cc < n / 32; cc += 2) {
+        const float* dci = dc + (size_t)(dc0 + cc * 32) * BM;
+        float dd[32];
+#pragma unroll
+        for (int k = 0; k < 32; ++k) dd[k] = dci[(size_t)k * BM];
+        float v[32];
+        tmem_ld32(tmem + b * 256 + lane_base + cc * 32, v);
+#pragma unroll
+        for (int k = 0; k < 32; ++k) v[k] *= dd[k];
+        act_store(act, r, cc * 32, v, with_lo);
+      }
+    };
     for (int w = blockIdx.x; w < p.ntiles && ok; w += gridDim.x) {
       const int row = p.tile_row[w] + r;
       const int sp = p.tile_species[w];
@@ -352,24 +407,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
         {
           const uint32_t b = job & 1;
           if (!(ok = take_acc(b))) break;
-          const float* bias = p.b1 + (size_t)g * p.d1;
-          for (int cc = half; cc < p.d1 / 32; cc += 2) {
-            float v[32];
-            tmem_ld32(tmem + b * 256 + lane_base + cc * 32, v);
-            float* dco = dc + (size_t)(cc * 32) * BM;
-#pragma unroll
-            for (int k = 0; k < 32; k += 4) {
-              const float4 bb = __ldg(reinterpret_cast<const float4*>(bias + cc * 32 + k));
-              const float zz[4] = {v[k] + bb.x, v[k + 1] + bb.y, v[k + 2] + bb.z, v[k + 3] + bb.w};
-#pragma unroll
-              for (int u = 0; u < 4; ++u) {
-                float dh;
-                celu_pair(zz[u], p.alpha, inv_alpha, v[k + u], dh);
-                dco[(size_t)(k + u) * BM] = dh;  // column-major: the warp writes 128 contiguous bytes
-              }
-            }
-            act_store(act, r, cc * 32, v, with_lo);
-          }
+          celu_layer(b, p.b1 + (size_t)g * p.d1, p.d1, 0);
           release_acc(b);
           publish_act();
         }
@@ -377,24 +415,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
         {
           const uint32_t b = job & 1;
           if (!(ok = take_acc(b))) break;
-          const float* bias = p.b2 + (size_t)g * p.d2;
-          for (int cc = half; cc < p.d2 / 32; cc += 2) {
-            float v[32];
-            tmem_ld32(tmem + b * 256 + lane_base + cc * 32, v);
-            float* dco = dc + (size_t)(p.d1 + cc * 32) * BM;
-#pragma unroll
-            for (int k = 0; k < 32; k += 4) {
-              const float4 bb = __ldg(reinterpret_cast<const float4*>(bias + cc * 32 + k));
-              const float zz[4] = {v[k] + bb.x, v[k + 1] + bb.y, v[k + 2] + bb.z, v[k + 3] + bb.w};
-#pragma unroll
-              for (int u = 0; u < 4; ++u) {
-                float dh;
-                celu_pair(zz[u], p.alpha, inv_alpha, v[k + u], dh);
-                dco[(size_t)(k + u) * BM] = dh;  // column-major: the warp writes 128 contiguous bytes
-              }
-            }
-            act_store(act, r, cc * 32, v, with_lo);
-          }
+          celu_layer(b, p.b2 + (size_t)g * p.d2, p.d2, p.d1);
           release_acc(b);
           publish_act();
         }
@@ -408,20 +429,25 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
           const float* w4 = p.w4 + (size_t)g * p.d3;
           float e = 0.f;
           for (int cc = half; cc < p.d3 / 32; cc += 2) {
+            float4 bb[8], ww[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+              bb[k] = __ldg(reinterpret_cast<const float4*>(bias + cc * 32) + k);
+              ww[k] = __ldg(reinterpret_cast<const float4*>(w4 + cc * 32) + k);
+            }
             float v[32];
             tmem_ld32(tmem + b * 256 + lane_base + cc * 32, v);
 #pragma unroll
-            for (int k = 0; k < 32; k += 4) {
-              const float4 bb = __ldg(reinterpret_cast<const float4*>(bias + cc * 32 + k));
-              const float4 ww = __ldg(reinterpret_cast<const float4*>(w4 + cc * 32 + k));
-              const float zz[4] = {v[k] + bb.x, v[k + 1] + bb.y, v[k + 2] + bb.z, v[k + 3] + bb.w};
-              const float wv[4] = {ww.x, ww.y, ww.z, ww.w};
+            for (int k = 0; k < 8; ++k) {
+              const float zz[4] = {v[4 * k] + bb[k].x, v[4 * k + 1] + bb[k].y, v[4 * k + 2] + bb[k].z,
+                                   v[4 * k + 3] + bb[k].w};
+              const float wv[4] = {ww[k].x, ww[k].y, ww[k].z, ww[k].w};
 #pragma unroll
               for (int u = 0; u < 4; ++u) {
                 float h, dh;
                 celu_pair(zz[u], p.alpha, inv_alpha, h, dh);
                 e = fmaf(h, wv[u], e);
-                v[k + u] = wv[u] * dh;
+                v[4 * k + u] = wv[u] * dh;
               }
             }
             act_store(act, r, cc * 32, v, with_lo);
@@ -446,14 +472,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
         {
           const uint32_t b = job & 1;
           if (!(ok = take_acc(b))) break;
-          for (int cc = half; cc < p.d2 / 32; cc += 2) {
-            float v[32];
-            tmem_ld32(tmem + b * 256 + lane_base + cc * 32, v);
-            const float* dci = dc + (size_t)(p.d1 + cc * 32) * BM;
-#pragma unroll
-            for (int k = 0; k < 32; ++k) v[k] *= dci[(size_t)k * BM];
-            act_store(act, r, cc * 32, v, with_lo);
-          }
+          mask_layer(b, p.d2, p.d1);
           release_acc(b);
           publish_act();
         }
@@ -461,50 +480,53 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
         {
           const uint32_t b = job & 1;
           if (!(ok = take_acc(b))) break;
-          for (int cc = half; cc < p.d1 / 32; cc += 2) {
-            float v[32];
-            tmem_ld32(tmem + b * 256 + lane_base + cc * 32, v);
-            const float* dci = dc + (size_t)(cc * 32) * BM;
-#pragma unroll
-            for (int k = 0; k < 32; ++k) v[k] *= dci[(size_t)k * BM];
-            act_store(act, r, cc * 32, v, with_lo);
-          }
+          mask_layer(b, p.d1, 0);
           release_acc(b);
           publish_act();
         }
-        // E6: dX chunks.  Each 32 x 32 block (32 rows of this warp, 32 columns)
-        // is transposed through a swizzled shared-memory tile so that every
-        // global store writes 128 contiguous bytes of one row.
+        // E6: dX chunks.  Each warp stages a 32 x 32 block (its 32 rows, 32
+        // columns) in its own shared-memory tile, in the 128-byte-swizzled
+        // layout of the dX tensor map, and the TMA engine writes it out: a bulk
+        // store for the first model, a bulk FP32 add in the L2 for the others.
+        // The lane that issues the copies first waits until its copies of the
+        // previous model have completed, so every element sums the models in
+        // model order.
+        if (lane == 0) bulk_wait_all();
+        __syncwarp();
+        uint8_t* tile = reinterpret_cast<uint8_t*>(xpose + (warp - 2) * 32 * 32);
+        uint8_t* trow = tile + lane * 128;
+        const int dx_row = p.tile_row[w] + 32 * q;
         for (int c = 0; c < p.d0 / 256 && ok; ++c) {
           const uint32_t b = job & 1;
           if (!(ok = take_acc(b))) break;
-          float* tile = xpose + (warp - 2) * 32 * 32;
           for (int cc = half; cc < 8; cc += 2) {
             float v[32];
             tmem_ld32(tmem + b * 256 + lane_base + cc * 32, v);
+            if (lane == 0) bulk_wait_read();  // the tile's previous copy has read it
+            __syncwarp();
 #pragma unroll
-            for (int k = 0; k < 32; ++k) tile[lane * 32 + (k ^ lane)] = v[k];
+            for (int j = 0; j < 8; ++j)
+              *reinterpret_cast<float4*>(trow + ((j ^ (lane & 7)) << 4)) =
+                  make_float4(v[4 * j] * p.inv_models, v[4 * j + 1] * p.inv_models, v[4 * j + 2] * p.inv_models,
+                              v[4 * j + 3] * p.inv_models);
+            fence_proxy_async();
             __syncwarp();
-            const int col = c * 256 + cc * 32 + lane;
-            const int row_base = p.tile_row[w] + 32 * q;
-#pragma unroll 8
-            for (int rr = 0; rr < 32; ++rr) {
-              const float val = tile[rr * 32 + (lane ^ rr)] * p.inv_models;
-              float* o = p.dx + (size_t)(row_base + rr) * p.d0 + col;
-              // later models add with fire-and-forget reductions (no load on the
-              // critical path); one thread owns each element, so the order of
-              // the sum over models is fixed
+            if (lane == 0) {
               if (m == 0)
-                *o = val;
+                tma_store_2d(&maps.dx, tile, c * 256 + cc * 32, dx_row);
               else
-                atomicAdd(o, val);
+                tma_add_2d(&maps.dx, tile, c * 256 + cc * 32, dx_row);
+              bulk_commit();
             }
-            __syncwarp();
           }
           release_acc(b);
         }
       }
     }
+    // the dX copies have completed (and no longer read shared memory) before
+    // the CTA exits
+    if (lane == 0) bulk_wait_all();
+    __syncwarp();
   }
   fence_before_sync();
   __syncthreads();
@@ -537,6 +559,19 @@ bool map2d(CUtensorMap* m, const void* base, uint64_t rows, uint64_t cols, uint3
   cuuint32_t estr[2] = {1, 1};
   return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// dX as FP32 [rows][cols] in 32 x 32 boxes (128-byte rows, 128-byte swizzle)
+bool map_dx(CUtensorMap* m, void* base, uint64_t rows, uint64_t cols) {
+  auto fn = encode_fn();
+  if (!fn || !base) return false;
+  cuuint64_t dims[2] = {cols, rows};
+  cuuint64_t strides[1] = {cols * 4};
+  cuuint32_t box[2] = {32, 32};
+  cuuint32_t estr[2] = {1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
@@ -582,7 +617,7 @@ int fnl_mlp_fused(int precision, int rows, int ntiles, const int* tile_species, 
             map2d(&maps.w3t, w->wt_hi[2], (uint64_t)G * d[3], d[2], d[3]) &&
             map2d(&maps.w3, w->w_hi[2], (uint64_t)G * d[2], d[3], d[2]) &&
             map2d(&maps.w2, w->w_hi[1], (uint64_t)G * d[1], d[2], d[1]) &&
-            map2d(&maps.w1, w->w_hi[0], (uint64_t)G * d[0], d[1], 256);
+            map2d(&maps.w1, w->w_hi[0], (uint64_t)G * d[0], d[1], 256) && map_dx(&maps.dx, dx, rows, d[0]);
   if (!ok) return FENNOL_ERR_CUDA;
   FusedParams p{};
   p.ntiles = ntiles;
