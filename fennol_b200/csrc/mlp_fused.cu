@@ -73,7 +73,7 @@ struct Maps {
 
 struct Bars {
   uint64_t x_full[kXStages], x_empty[kXStages], w_full[kWStages], w_empty[kWStages];
-  uint64_t acc_full[2], acc_free[2], act_ready, act_free, done, ex_ready, ex_free;
+  uint64_t acc_full[2], acc_free[2], act_ready[4], act_free, done, ex_ready, ex_free;
   uint32_t tmem_slot;
   int abort_flag;
   float ex[BM];
@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
       mbar_init(&bars->w_full[s], 1);
       mbar_init(&bars->w_empty[s], 1);
     }
-    mbar_init(&bars->act_ready, kEpiThreads);
+    for (int a = 0; a < 4; ++a) mbar_init(&bars->act_ready[a], kEpiThreads);
     mbar_init(&bars->act_free, 1);
     mbar_init(&bars->done, 1);
     mbar_init(&bars->ex_ready, kEpiThreads / 2);
@@ -238,7 +238,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
   } else if (warp == 1) {
     // ------------------------------------------------------------------ MMA issuer
     if (lane == 0) {
-      uint32_t xq = 0, wq = 0, act_phase = 0;
+      uint32_t xq = 0, wq = 0;
+      uint32_t act_phase[4] = {0, 0, 0, 0};
       uint32_t nuse[2] = {0, 0};
       uint32_t job = 0;
       bool ok = true;
@@ -247,11 +248,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
         if (nuse[b] == 0) return true;
         return wait_bar(&bars->acc_free[b], (nuse[b] - 1) & 1, abort_flag, p.err);
       };
-      // one GEMM whose A operand is the activation buffer (K/64 atoms) and B the weight ring
-      auto gemm_act = [&](int n, int k, uint32_t b) -> bool {
+      // one GEMM whose A operand is the activation buffer (K/64 atoms) and B the
+      // weight ring.  With wait_act, each K-atom is used as soon as the epilogue
+      // has published it, so the GEMM overlaps the epilogue that feeds it.
+      auto gemm_act = [&](int n, int k, uint32_t b, bool wait_act) -> bool {
         const uint32_t idesc = idesc_bf16_f32(n);
         const uint32_t d = tmem + b * 256;
         for (int kc = 0; kc < k / BK; ++kc, ++wq) {
+          if (wait_act) {
+            if (!wait_bar(&bars->act_ready[kc], act_phase[kc] & 1, abort_flag, p.err)) return false;
+            ++act_phase[kc];
+          }
           const int s = wq % kWStages;
           if (!wait_bar(&bars->w_full[s], (wq / kWStages) & 1, abort_flag, p.err)) return false;
           fence_after_sync();
@@ -296,25 +303,19 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
           const int ns[4] = {p.d2, p.d3, p.d2, p.d1};
           const int ks[4] = {p.d1, p.d2, p.d3, p.d2};
           for (int jb = 0; jb < 4 && ok; ++jb) {
-            if (!(ok = wait_bar(&bars->act_ready, act_phase & 1, abort_flag, p.err))) break;
-            ++act_phase;
-            fence_after_sync();
             const uint32_t b = job & 1;
             if (!(ok = acquire_acc(b))) break;
-            if (!(ok = gemm_act(ns[jb], ks[jb], b))) break;
+            if (!(ok = gemm_act(ns[jb], ks[jb], b, true))) break;
             mma_commit(&bars->acc_full[b]);
             ++nuse[b];
             ++job;
           }
           if (!ok) break;
-          // B1: dX chunks of 256 columns, A = G1
-          if (!(ok = wait_bar(&bars->act_ready, act_phase & 1, abort_flag, p.err))) break;
-          ++act_phase;
-          fence_after_sync();
+          // B1: dX chunks of 256 columns, A = G1 (published atom by atom for the first)
           for (int c = 0; c < p.d0 / 256 && ok; ++c) {
             const uint32_t b = job & 1;
             if (!(ok = acquire_acc(b))) break;
-            if (!(ok = gemm_act(256, p.d1, b))) break;
+            if (!(ok = gemm_act(256, p.d1, b, c == 0))) break;
             mma_commit(&bars->acc_full[b]);
             ++nuse[b];
             ++job;
@@ -352,9 +353,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
       ++nuse[b];
       ++job;
     };
-    auto publish_act = [&]() {
+    // the 32 columns of K-atom a written by this thread are visible to the MMA
+    // (async proxy); the atom is complete when all epilogue threads arrived
+    auto publish_atom = [&](int a) {
       fence_proxy_async();
-      mbar_arrive(&bars->act_ready);
+      mbar_arrive(&bars->act_ready[a]);
     };
     // H = celu(Z + bias) -> act for columns [0, n); celu'(z) -> dc columns
     // [dc0, dc0 + n).  The bias loads are issued before the TMEM load so that
@@ -379,6 +382,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
           }
         }
         act_store(act, r, cc * 32, v, with_lo);
+        publish_atom(cc >> 1);
       }
     };
     // G = D * celu'(z) -> act for columns [0, n), celu' read back from dc
@@ -395,6 +399,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
 #pragma unroll
         for (int k = 0; k < 32; ++k) v[k] *= dd[k];
         act_store(act, r, cc * 32, v, with_lo);
+        publish_atom(cc >> 1);
       }
     };
     for (int w = blockIdx.x; w < p.ntiles && ok; w += gridDim.x) {
@@ -409,7 +414,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
           if (!(ok = take_acc(b))) break;
           celu_layer(b, p.b1 + (size_t)g * p.d1, p.d1, 0);
           release_acc(b);
-          publish_act();
         }
         // E2: H2 = celu(Z2 + b2) -> act; celu'(z2) -> dc[d1:d1+d2]
         {
@@ -417,7 +421,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
           if (!(ok = take_acc(b))) break;
           celu_layer(b, p.b2 + (size_t)g * p.d2, p.d2, p.d1);
           release_acc(b);
-          publish_act();
         }
         // E3: energy head; G3 = w4 * celu'(z3) -> act.  Both column halves work;
         // the half-1 partial energy of each row reaches the half-0 thread through
@@ -451,6 +454,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
               }
             }
             act_store(act, r, cc * 32, v, with_lo);
+            publish_atom(cc >> 1);
           }
           release_acc(b);
           if (half == 1) {
@@ -466,7 +470,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
             if (m == M - 1) p.e_rows[row] = e_row;
           }
           ++ex_phase;
-          publish_act();
         }
         // E4: G2 = D2 * celu'(z2) -> act
         {
@@ -474,7 +477,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
           if (!(ok = take_acc(b))) break;
           mask_layer(b, p.d2, p.d1);
           release_acc(b);
-          publish_act();
         }
         // E5: G1 = D1 * celu'(z1) -> act
         {
@@ -482,7 +484,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
           if (!(ok = take_acc(b))) break;
           mask_layer(b, p.d1, 0);
           release_acc(b);
-          publish_act();
         }
         // E6: dX chunks.  Each warp stages a 32 x 32 block (its 32 rows, 32
         // columns) in its own shared-memory tile, in the 128-byte-swizzled
