@@ -139,11 +139,13 @@ def make_engine(workload, precision, device, seed=0, bf16_weights=True, output_s
 
 
 def time_steps(eng, steps, warmup, flush):
-    """Per-step device times (ms) of graph-replayed MD steps, L2 flushed between steps."""
+    """Per-step device times (ms) of graph-replayed MD steps, L2 flushed
+    between steps, and the number of list rebuilds inside the timed steps."""
     import torch
 
     eng.run(warmup)  # also regrows lists if needed
     graph = eng._graph_for(None, 1)
+    rebuilds0 = eng.rebuild_count()
     stream = torch.cuda.current_stream()
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
@@ -158,7 +160,7 @@ def time_steps(eng, steps, warmup, flush):
     if eng._regrow():  # an overflow during timing: lists regrown, time again
         return time_steps(eng, steps, 0, flush)
     eng.step_count += steps
-    return np.array([s.elapsed_time(e) for s, e in zip(starts, ends)])
+    return np.array([s.elapsed_time(e) for s, e in zip(starts, ends)]), eng.rebuild_count() - rebuilds0
 
 
 def time_mlp(pot, eng, reps):
@@ -332,7 +334,7 @@ def ensemble_98k(device, steps, warmup, flush):
     out = {"workload": w["desc"], "atoms": 0, "models": w["n_models"]}
     for precision in ("bf16x2", "fp32"):
         box, pot, eng = make_engine("water98k", precision, device)
-        ms = time_steps(eng, steps, warmup, flush)
+        ms, _ = time_steps(eng, steps, warmup, flush)
         mlp_ms = time_mlp(pot, eng, 5)
         flops = MLP_FLOP_PER_ATOM * box.natoms * w["n_models"]
         out["atoms"] = box.natoms
@@ -528,7 +530,7 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clocks:
-        ms = time_steps(eng, args.steps, args.warmup, flush)
+        ms, rebuilds = time_steps(eng, args.steps, args.warmup, flush)
     total_ms = float(ms.sum())
     if world > 1:
         from fennol_b200.replicas import max_over_ranks
@@ -551,8 +553,8 @@ def main():
                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
            "latency_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99))},
            "clocks": clocks.summary(),
-           "gpu_launches": eng.launches_per_step() * args.steps,
-           "rebuilds_in_run": eng.rebuild_count()}
+           "gpu_launches": eng.launches_per_step() * args.steps + eng.rebuild_launches() * rebuilds,
+           "rebuilds_in_run": rebuilds}
     # end-to-end public-API calls on every rank; the job rate uses the slowest rank
     e2e_res = e2e(pot, box, max(5, args.steps // 3), 3)
     if world > 1:
@@ -603,7 +605,7 @@ def main():
                                                             kd.get("algorithmic_flop_per_launch"))}
         if precision != "fp32" and extras:
             _, pot32, eng32 = make_engine(args.workload, "fp32", device, seed=rank)
-            ms32 = time_steps(eng32, max(5, args.steps // 3), 3, flush)
+            ms32, _ = time_steps(eng32, max(5, args.steps // 3), 3, flush)
             v32 = box.natoms / (float(ms32.mean()) * 1e-3)
             res["fp32_form"] = {"value": v32, "ms_per_step": float(ms32.mean()),
                                 "mlp_ms_per_launch": time_mlp(pot32, eng32, 10)}

@@ -97,6 +97,8 @@ _SIGNATURES = {
     "fennol_md_step_systems": (I, [I, I, D, P, P, P, P, D, D, P, P, P, P, P, P, P, P, P, D, P, P]),
     "fennol_md_mark_rebuilt": (I, [I, P, P, P, P]),
     "fennol_md_kinetic": (I, [I, P, P, P, P]),
+    "fennol_capture_if_begin": (I, [P, P, P]),
+    "fennol_capture_if_end": (I, [P]),
 }
 
 _lib: Optional[C.CDLL] = None

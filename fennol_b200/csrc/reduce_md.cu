@@ -14,26 +14,39 @@ using namespace fnl;
 
 namespace {
 
-// Two-level fixed-order reduction: every block sums a contiguous chunk of
-// one system's atoms into partial[b*chunks + c]; one warp per system then
-// adds the partials in order.  Deterministic for a given batch layout.
+// Fixed-order reduction in one launch.  System b (atoms sys_start[b] ..
+// sys_start[b+1]) is cut into C_b = max(1, ceil(n_b / 1024)) chunks that start
+// at its first atom; chunk c of system b owns the slot
+//     base(b) + c,   base(b) = b + floor(sys_start[b] / 1024).
+// base() is strictly increasing and base(b) + C_b <= base(b + 1), so slots
+// are distinct without a prefix sum; a block finds the system of a slot by
+// binary search on sys_start alone (slots past C_b are gaps).  Blocks write
+// one float64 partial per chunk; the last block to finish (ticket counter)
+// adds each system's partials in chunk order.  The result depends only on a
+// system's own atoms, not on the rest of the batch.
 constexpr int kRedChunk = 1024;
 
-__global__ void k_energy_partial(const float* __restrict__ e_rows, const int* __restrict__ atom_row,
-                                 const int* __restrict__ sys_start, const int* __restrict__ chunk_off,
-                                 int nsys, double scale, double* __restrict__ partial,
-                                 double* __restrict__ e_atom) {
+__device__ __forceinline__ int red_base(const int* sys_start, int b) { return b + sys_start[b] / kRedChunk; }
+__device__ __forceinline__ int red_chunks(const int* sys_start, int b) {
+  return max(1, (sys_start[b + 1] - sys_start[b] + kRedChunk - 1) / kRedChunk);
+}
+
+__global__ void __launch_bounds__(256) k_energy_sum(const float* __restrict__ e_rows, const int* __restrict__ atom_row,
+                                                   const int* __restrict__ sys_start, int nsys, int nslots, double scale,
+                                                   double* __restrict__ partial, double* __restrict__ e_atom,
+                                                   double* __restrict__ energy, unsigned* __restrict__ ticket) {
   pdl_wait();
   __shared__ double part[256];
-  const int total = chunk_off[nsys];
-  for (int w = blockIdx.x; w < total; w += gridDim.x) {
-    // system b with chunk_off[b] <= w < chunk_off[b+1] (binary search)
+  __shared__ bool last;
+  for (int w = blockIdx.x; w < nslots; w += gridDim.x) {
+    // the system b with base(b) <= w < base(b + 1)
     int lo = 0, hi = nsys - 1;
     while (lo < hi) {
       int mid = (lo + hi + 1) >> 1;
-      if (chunk_off[mid] <= w) lo = mid; else hi = mid - 1;
+      if (red_base(sys_start, mid) <= w) lo = mid; else hi = mid - 1;
     }
-    const int b = lo, c = w - chunk_off[b];
+    const int b = lo, c = w - red_base(sys_start, b);
+    if (c < 0 || c >= red_chunks(sys_start, b)) continue;  // a gap slot (uniform per block)
     const int i0 = sys_start[b] + c * kRedChunk;
     const int i1 = min(i0 + kRedChunk, sys_start[b + 1]);
     double s = 0.0;
@@ -51,59 +64,19 @@ __global__ void k_energy_partial(const float* __restrict__ e_rows, const int* __
     if (threadIdx.x == 0) partial[w] = part[0];
     __syncthreads();
   }
-}
-
-__global__ void k_energy_final(const int* __restrict__ chunk_off, int nsys, const double* __restrict__ partial,
-                               double* __restrict__ energy) {
-  pdl_wait();
-  int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= nsys) return;
-  double s = 0.0;
-  for (int k = chunk_off[b]; k < chunk_off[b + 1]; ++k) s += partial[k];
-  energy[b] = s;
-}
-
-// chunk_off[b] = sum_{b' < b} max(1, ceil(n_b' / kRedChunk)) (one block, tiled scan).
-__global__ void k_chunk_offsets(const int* __restrict__ sys_start, int nsys, int* __restrict__ chunk_off) {
-  pdl_wait();
-  __shared__ int warp_sums[32];
-  __shared__ int carry;
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  if (tid == 0) carry = 0;
+  // the last block to arrive sums the partials (all written before its ticket)
+  __threadfence();
+  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
   __syncthreads();
-  for (int base = 0; base < nsys; base += blockDim.x) {
-    int b = base + tid;
-    int v = 0;
-    if (b < nsys) {
-      int n = sys_start[b + 1] - sys_start[b];
-      v = max(1, (n + kRedChunk - 1) / kRedChunk);
-    }
-    int incl = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      int t = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += t;
-    }
-    if (lane == 31) warp_sums[wid] = incl;
-    __syncthreads();
-    if (wid == 0) {
-      int nw = blockDim.x >> 5;
-      int s = lane < nw ? warp_sums[lane] : 0;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        int t = __shfl_up_sync(0xffffffffu, s, o);
-        if (lane >= o) s += t;
-      }
-      if (lane < nw) warp_sums[lane] = s;
-    }
-    __syncthreads();
-    int excl = carry + (wid > 0 ? warp_sums[wid - 1] : 0) + incl - v;
-    if (b < nsys) chunk_off[b] = excl;
-    __syncthreads();
-    if (tid == blockDim.x - 1) carry = excl + v;
-    __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int b = threadIdx.x; b < nsys; b += blockDim.x) {
+    const int base = red_base(sys_start, b), nc = red_chunks(sys_start, b);
+    double s = 0.0;
+    for (int k = 0; k < nc; ++k) s += __ldcg(partial + base + k);
+    energy[b] = s;
   }
-  if (tid == 0) chunk_off[nsys] = carry;
+  if (threadIdx.x == 0) *ticket = 0u;  // ready for the next call
 }
 
 __global__ void k_forces_finalize(const float4* __restrict__ f4, int n, float scale, float* __restrict__ f) {
@@ -277,8 +250,8 @@ __global__ void k_kinetic(int n, const double* __restrict__ v, const double* __r
 
 extern "C" size_t fennol_energy_workspace_bytes(int natoms, int nsys) {
   if (natoms < 0 || nsys < 0) return 0;
-  size_t chunks = (size_t)natoms / kRedChunk + (size_t)nsys + 1;
-  return 256 + (size_t)(nsys + 1) * sizeof(int) + 256 + chunks * sizeof(double);
+  size_t slots = (size_t)natoms / kRedChunk + (size_t)nsys + 1;
+  return 256 + slots * sizeof(double);
 }
 
 // Per-system sum of per-centre virials, fixed order (one block per system).
@@ -325,16 +298,13 @@ extern "C" int fennol_energy_reduce(const float* e_rows, const int* atom_row, in
   if (!sys_start || !energy || !workspace || (natoms > 0 && (!e_rows || !atom_row))) return FENNOL_ERR_INVALID;
   if (workspace_bytes < fennol_energy_workspace_bytes(natoms, nsys)) return FENNOL_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
-  int* chunk_off = (int*)workspace;
-  double* partial = (double*)((char*)workspace + ((sizeof(int) * (size_t)(nsys + 1) + 255) / 256 * 256));
-  FNL_LAUNCH_PDL(k_chunk_offsets, 1, 1024, 0, st, sys_start, nsys, chunk_off);
-  FNL_CHECK_LAUNCH();
-  int blocks = natoms / kRedChunk + nsys;
-  if (blocks > 4 * 148) blocks = 4 * 148;
-  FNL_LAUNCH_PDL(k_energy_partial, blocks, 256, 0, st, e_rows, atom_row, sys_start, chunk_off, nsys, scale, partial,
-                                           e_atom);
-  FNL_CHECK_LAUNCH();
-  FNL_LAUNCH_PDL(k_energy_final, (nsys + 127) / 128, 128, 0, st, chunk_off, nsys, partial, energy);
+  unsigned* ticket = (unsigned*)workspace;
+  double* partial = (double*)((char*)workspace + 256);
+  // slots: base(nsys - 1) + C_{nsys-1} <= nsys + natoms / 1024 + 1
+  const int nslots = natoms / kRedChunk + nsys + 1;
+  const int blocks = nslots < 4 * 148 ? nslots : 4 * 148;
+  FNL_LAUNCH_PDL(k_energy_sum, blocks, 256, 0, st, e_rows, atom_row, sys_start, nsys, nslots, scale, partial, e_atom,
+                 energy, ticket);
   FNL_CHECK_LAUNCH();
   return FENNOL_OK;
 }

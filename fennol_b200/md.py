@@ -28,7 +28,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import call
+from ._lib import ERR_UNSUPPORTED, FennolError, call, load
 from .params import atomic_masses
 from .potential import ANIPotential, GraphBuffers, HARTREE_TO_KCALMOL, _ptr
 
@@ -41,6 +41,33 @@ _K_B = 3.166811563e-6
 _KCALPERMOL = 627.5096080305927
 MASS_DA_TO_MD = _MPROT * _KCALPERMOL * _PS ** 2 / _ANGSTROM ** 2   # Da -> kcal/mol ps^2 / A^2
 KB_KCALMOL = _K_B * _KCALPERMOL                                    # kcal/mol/K
+
+
+# number of rebuilds captured as conditional graph nodes (diagnostics, tests)
+conditional_captures = 0
+
+
+def launch_flagged_rebuild(g: GraphBuffers, layout, coords, status, flag, x, x_ref, stream: int,
+                           body_stream: int):
+    """Enqueue the displacement-triggered list rebuild (build, then x_ref = x
+    and flag = 0).  While ``stream`` is being captured the rebuild becomes the
+    body of a conditional node (captured on ``body_stream``) that a replay runs
+    only when the device flag is set; uncaptured, the rebuild kernels read the
+    flag and return at once when it is clear."""
+    global conditional_captures
+    rc = load().fennol_capture_if_begin(stream, flag.data_ptr(), body_stream)
+    if rc == ERR_UNSUPPORTED:  # not capturing
+        body_stream = stream
+    elif rc != 0:
+        raise FennolError("fennol_capture_if_begin", rc)
+    else:
+        conditional_captures += 1
+    try:
+        g.build(layout, coords, status, body_stream, enable_flag=flag)
+        call("fennol_md_mark_rebuilt", layout.n, x.data_ptr(), x_ref.data_ptr(), flag.data_ptr(), body_stream)
+    finally:
+        if body_stream != stream:
+            call("fennol_capture_if_end", body_stream)
 
 
 class MDEngine:
@@ -105,6 +132,8 @@ class MDEngine:
         self.force_scale = HARTREE_TO_KCALMOL / pot.unit_scale
         self.graph_buf, self.ws = pot.buffers(self.layout, skin=self.skin)
         self._graphs = {}
+        # captures the rebuild kernels into the body of the step graph's IF node
+        self._body_stream = torch.cuda.Stream(dev)
         self._snapshot = None
         self.rebuilds = 0
         self._initial_forces()
@@ -138,7 +167,10 @@ class MDEngine:
 
     def _launch_step(self, st, rebuild: Optional[bool]):
         """Enqueue one MD step.  rebuild: True/False (stride mode) or None
-        (device displacement trigger)."""
+        (device displacement trigger).  Under graph capture the displacement
+        rebuild is the body of a conditional node that runs only when the flag
+        is set; otherwise the rebuild kernels read the flag and return at once
+        when it is clear."""
         g, ws, lay = self.graph_buf, self.ws, self.layout
         use_flag = rebuild is None
         call("fennol_md_step", self.n, self.dt, self.x.data_ptr(), self.v.data_ptr(),
@@ -148,24 +180,28 @@ class MDEngine:
              self.x_ref.data_ptr() if use_flag else None, 0.5 * self.skin,
              self.flag.data_ptr() if use_flag else None, st)
         if use_flag:
-            g.build(lay, self.coords, ws.status, st, enable_flag=self.flag)
-            call("fennol_md_mark_rebuilt", self.n, self.x.data_ptr(), self.x_ref.data_ptr(),
-                 self.flag.data_ptr(), st)
+            launch_flagged_rebuild(g, lay, self.coords, ws.status, self.flag, self.x, self.x_ref, st,
+                                   self._body_stream.cuda_stream)
         elif rebuild:
             g.build(lay, self.coords, ws.status, st)
         g.filter(lay, self.coords, ws.status, st)
         self.pot.launch_forces(lay, g, ws, st, True)
 
     def launches_per_step(self) -> int:
-        """Kernels of this library enqueued by one step (rebuild kernels
-        included; they return at once when no rebuild is due)."""
+        """Kernels of this library that one graph-replayed step without a
+        rebuild runs (displacement trigger: the flag-to-condition kernel; the
+        rebuild kernels are in the conditional body, see rebuild_launches)."""
         n = 2  # md step + counter
         if self.trigger == "displacement":
-            # prepare/scan/scatter/sort cells/cells/allpairs + mark/clear
-            n += (6 if self.graph_buf.ncells > 0 else 2) + 2
+            n += 1
         n += 1 if self.skin > 0 else 0
-        n += 1 + self.pot.mlp_launches() + 3 + 1  # aev fwd, mlp, energy sum (3), aev bwd
+        n += 1 + self.pot.mlp_launches() + 1 + 1  # aev fwd, mlp, energy sum, aev bwd
         return n
+
+    def rebuild_launches(self) -> int:
+        """Kernels of the rebuild body (prepare/scan/scatter/sort cells/cells/
+        allpairs + mark/clear)."""
+        return (6 if self.graph_buf.ncells > 0 else 2) + 2
 
     # ---------------------------------------------------------------- graphs
     def _graph_for(self, rebuild: Optional[bool], nsteps: int):

@@ -43,7 +43,7 @@ import torch
 
 from . import _lib
 from ._lib import call
-from .md import KB_KCALMOL, MASS_DA_TO_MD
+from .md import KB_KCALMOL, MASS_DA_TO_MD, launch_flagged_rebuild
 from .params import atomic_masses
 from .potential import (MAX_ROW, ANIPotential, BatchLayout, GraphBuffers, HARTREE_TO_KCALMOL,
                         Workspace, _ptr, min_image_ok)
@@ -206,6 +206,7 @@ class _MDLane:
     def __init__(self, engine: "ServingEngine"):
         self.e = engine
         self.stream = torch.cuda.Stream(engine.device)
+        self.body_stream = torch.cuda.Stream(engine.device)  # conditional rebuild bodies
         self.members: List[dict] = []
         self.ready: List[tuple] = []
         self.ready_event: Optional[torch.cuda.Event] = None
@@ -290,9 +291,8 @@ class _MDLane:
              lay.t_atom_sys.data_ptr(), lay.t_sys_start.data_ptr(), st["sys_seed"].data_ptr(),
              st["sys_step"].data_ptr(), st["coords"].data_ptr(), lay.t_species.data_ptr(),
              ws.xyzs.data_ptr(), st["x_ref"].data_ptr(), 0.5 * e.skin, st["flag"].data_ptr(), s)
-        g.build(lay, st["coords"], ws.status, s, enable_flag=st["flag"])
-        call("fennol_md_mark_rebuilt", b.n, st["x"].data_ptr(), st["x_ref"].data_ptr(),
-             st["flag"].data_ptr(), s)
+        launch_flagged_rebuild(g, lay, st["coords"], ws.status, st["flag"], st["x"], st["x_ref"], s,
+                               self.body_stream.cuda_stream)
         g.filter(lay, st["coords"], ws.status, s)
         pot.launch_forces(lay, g, ws, s, True)
 

@@ -301,15 +301,18 @@ int fennol_mlp_energy_grad(int precision, int rows, int ntiles, const int* tile_
 /* Reductions and outputs                                                    */
 /* ------------------------------------------------------------------------ */
 
-/* Workspace of fennol_energy_reduce, in bytes. */
+/* Workspace of fennol_energy_reduce, in bytes.  It must be zero-filled
+ * before its first use; every call leaves it ready for the next one. */
 size_t fennol_energy_workspace_bytes(int natoms, int nsys);
 
 /*
  * Per-system energies in float64: energy[b] = scale * sum_{i in b}
- * e_rows[atom_row[i]] (fixed summation order: 1024-atom chunks, then the
- * chunk sums in order).  Replaces the segment_sum of FENNIX.total_energy
- * (fennix.py:218-258).  e_atom (float64 [natoms], may be NULL) receives
- * scale * per-atom energies in input order.
+ * e_rows[atom_row[i]] (fixed summation order: 1024-atom chunks from the
+ * system's first atom, then the chunk sums in order, so a system's energy
+ * does not depend on the other systems of the batch).  One kernel launch.
+ * Replaces the segment_sum of FENNIX.total_energy (fennix.py:218-258).
+ * e_atom (float64 [natoms], may be NULL) receives scale * per-atom energies
+ * in input order.  Calls that share a workspace must be stream-ordered.
  */
 int fennol_energy_reduce(const float* e_rows, const int* atom_row, int natoms,
                          const int* sys_start, int nsys, double scale, double* energy,
@@ -368,6 +371,23 @@ int fennol_md_step_systems(int natoms, int nsys, double dt, double* x, double* v
 /* After a rebuild: x_ref = x and *rebuild_flag = 0 (both device). */
 int fennol_md_mark_rebuilt(int natoms, const double* x, double* x_ref, int* rebuild_flag,
                            void* stream);
+
+/*
+ * Conditional neighbour-list update inside a CUDA graph of MD steps.  The
+ * reference decides between a full rebuild and a skin update on the host
+ * every step (md/integrate.py:515-565); these two calls let a captured step
+ * make that decision on the device from the displacement flag that
+ * fennol_md_step sets.  While `stream` is being captured,
+ * fennol_capture_if_begin enqueues a one-thread kernel that copies
+ * (*flag != 0) into the condition of an IF node added after it; the work the
+ * caller then enqueues on `body_stream` (its own stream, not capturing) until
+ * fennol_capture_if_end is captured into the body of that node, which a
+ * replay runs only when the flag was set.  Work enqueued on `stream` after
+ * fennol_capture_if_begin depends on the IF node.  Returns
+ * FENNOL_ERR_UNSUPPORTED (enqueuing nothing) when `stream` is not capturing.
+ */
+int fennol_capture_if_begin(void* stream, const int* flag, void* body_stream);
+int fennol_capture_if_end(void* body_stream);
 
 /* kinetic[0] = 0.5 * sum m v^2 (float64, deterministic order). */
 int fennol_md_kinetic(int natoms, const double* v, const double* inv_mass, double* kinetic,

@@ -95,3 +95,29 @@ def test_overflow_rolls_back_and_regrows(gentle):
     ref.run(20)
     assert eng.graph_buf.cap_r > 24
     assert np.abs(eng.x.cpu().numpy() - ref.x.cpu().numpy()).max() < 1e-6
+
+
+def test_conditional_rebuild_graph_matches_uncaptured_steps(gentle):
+    """Graph-replayed steps hold the displacement rebuild in a conditional node;
+    steps launched without capture run the flag-gated rebuild kernels.  Both
+    rebuild at the same steps; positions agree to float32 summation-order
+    noise (force atomics), which the dynamics amplify over longer runs."""
+    s = water_box(6, seed=26)
+    a = MDEngine(gentle, s.coordinates, s.species, s.cell, thermostat="NVE", skin=0.2, seed=8,
+                 check_every=400)
+    b = MDEngine(gentle, s.coordinates, s.species, s.cell, thermostat="NVE", skin=0.2, seed=8,
+                 check_every=400)
+    r_a0, r_b0 = a.rebuild_count(), b.rebuild_count()
+    st = torch.cuda.current_stream().cuda_stream
+    # (steps, position tolerance, allowed rebuild-count difference): after 300
+    # steps the grown noise may move one trigger by a step
+    for steps, tol, drb in ((30, 1e-6, 0), (270, 1e-3, 1)):
+        a.run(steps, graph_steps=3)
+        for _ in range(steps):
+            b._launch_step(st, None)
+        torch.cuda.synchronize()
+        assert a.pot.check_status(a.ws, a.graph_buf) is None
+        assert b.pot.check_status(b.ws, b.graph_buf) is None
+        ra, rb = a.rebuild_count() - r_a0, b.rebuild_count() - r_b0
+        assert ra >= 1 and abs(ra - rb) <= drb
+        assert np.abs(a.x.cpu().numpy() - b.x.cpu().numpy()).max() < tol
