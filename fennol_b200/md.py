@@ -8,8 +8,13 @@ skin update, ``:515-566``) -> ``update_observables`` (energy and forces,
 * positions and velocities are float64 on the device (the reference keeps
   the precision of ``fprec``); forces come from the float32/BF16 kernels;
 * the neighbour list is rebuilt when an atom moved more than half the skin
-  since the last rebuild (a device flag), or every ``nblist_stride`` steps
-  like the reference (``integrate.py:498-510``) when ``trigger="stride"``;
+  since the last rebuild (``trigger="displacement"``: a device flag, the
+  rebuild a conditional node of the step graph), or every ``nblist_stride``
+  steps like the reference (``integrate.py:498-510``) when
+  ``trigger="stride"``.  In stride mode every step between rebuilds also
+  checks the displacements on the device; a chunk in which an atom moved more
+  than half the skin is rolled back and replayed with a shorter stride, so
+  no kept step ran on a stale list (the reference trusts its stride);
 * every step is captured once in a CUDA graph and replayed; capacity
   overflow (the reference's ``check_reallocate``) is detected from the device
   status words every ``check_every`` steps and answered by restoring the last
@@ -96,6 +101,8 @@ class MDEngine:
             # integrate.py:498-507: 2 A of skin lasts 40 fs at 300 K
             nblist_stride = max(1, int(math.floor(self.skin / 2.0 * 40.0 / dt_fs))) if skin > 0 else 1
         self.nblist_stride = nblist_stride
+        self.stride_reductions = 0
+        self.verify_stride = trigger == "stride" and self.skin > 0
         self.check_every = check_every
         mass_da = atomic_masses(species)
         mass = mass_da * MASS_DA_TO_MD
@@ -173,17 +180,20 @@ class MDEngine:
         when it is clear."""
         g, ws, lay = self.graph_buf, self.ws, self.layout
         use_flag = rebuild is None
+        check = use_flag or (self.verify_stride and not rebuild)
         call("fennol_md_step", self.n, self.dt, self.x.data_ptr(), self.v.data_ptr(),
              self.inv_mass.data_ptr(), ws.forces4.data_ptr(), self.force_scale, self.a1,
              _ptr(self.a2), self.seed, self.step_counter.data_ptr(),
              self.coords.data_ptr(), lay.t_species.data_ptr(), ws.xyzs.data_ptr(),
-             self.x_ref.data_ptr() if use_flag else None, 0.5 * self.skin,
-             self.flag.data_ptr() if use_flag else None, st)
+             self.x_ref.data_ptr() if check else None, 0.5 * self.skin,
+             self.flag.data_ptr() if check else None, st)
         if use_flag:
             launch_flagged_rebuild(g, lay, self.coords, ws.status, self.flag, self.x, self.x_ref, st,
                                    self._body_stream.cuda_stream)
         elif rebuild:
             g.build(lay, self.coords, ws.status, st)
+            if self.verify_stride:
+                self.x_ref.copy_(self.x)  # the stream is torch's current one (captured or not)
         g.filter(lay, self.coords, ws.status, st)
         self.pot.launch_forces(lay, g, ws, st, True)
 
@@ -199,9 +209,28 @@ class MDEngine:
         return n
 
     def rebuild_launches(self) -> int:
-        """Kernels of the rebuild body (prepare/scan/scatter/sort cells/cells/
-        allpairs + mark/clear)."""
-        return (6 if self.graph_buf.ncells > 0 else 2) + 2
+        """Kernels a rebuild adds to a step: prepare/scan/scatter/sort cells/
+        cells/allpairs (+ mark/clear with the displacement trigger)."""
+        return (6 if self.graph_buf.ncells > 0 else 2) + (2 if self.trigger == "displacement" else 0)
+
+    def graph_for_step(self, k: int):
+        """The one-step graph of the k-th step from now."""
+        if self.trigger == "displacement":
+            return self._graph_for(None, 1)
+        return self._graph_for((self.step_count + k) % self.nblist_stride == 0, 1)
+
+    def displaced_beyond_skin(self) -> bool:
+        """Stride mode: did an atom move more than half the skin since its
+        list was built, in a step that did not rebuild?"""
+        return self.verify_stride and bool(int(self.flag.item()))
+
+    def shorten_stride(self):
+        """Roll back to the last snapshot, rebuild there and continue with a
+        shorter stride (3/4 of it)."""
+        self.restore()
+        self.nblist_stride = max(1, (3 * self.nblist_stride) // 4)
+        self.stride_reductions += 1
+        self._initial_forces_from_current()
 
     # ---------------------------------------------------------------- graphs
     def _graph_for(self, rebuild: Optional[bool], nsteps: int):
@@ -268,6 +297,9 @@ class MDEngine:
                     k += 1
             if self._regrow():
                 continue  # replay the chunk with larger lists
+            if self.displaced_beyond_skin():
+                self.shorten_stride()
+                continue  # replay the chunk with more frequent rebuilds
             self.step_count += chunk
             done += chunk
             self.snapshot()

@@ -121,3 +121,19 @@ def test_conditional_rebuild_graph_matches_uncaptured_steps(gentle):
         ra, rb = a.rebuild_count() - r_a0, b.rebuild_count() - r_b0
         assert ra >= 1 and abs(ra - rb) <= drb
         assert np.abs(a.x.cpu().numpy() - b.x.cpu().numpy()).max() < tol
+
+
+def test_checked_stride_rolls_back_a_too_long_stride(gentle):
+    """Stride mode checks every step's displacement on the device: a stride far
+    too long for the skin is caught, the chunk replayed with shorter strides,
+    and the trajectory matches the displacement-triggered one."""
+    s = water_box(5, seed=27)
+    a = MDEngine(gentle, s.coordinates, s.species, s.cell, thermostat="NVE", skin=0.3, seed=9,
+                 trigger="stride", nblist_stride=500, check_every=20)
+    b = MDEngine(gentle, s.coordinates, s.species, s.cell, thermostat="NVE", skin=0.3, seed=9,
+                 check_every=20)
+    a.run(40)
+    b.run(40)
+    assert a.stride_reductions >= 1 and a.nblist_stride < 500
+    assert not a.displaced_beyond_skin()
+    assert np.abs(a.x.cpu().numpy() - b.x.cpu().numpy()).max() < 1e-5
