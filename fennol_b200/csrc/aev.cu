@@ -194,17 +194,25 @@ __device__ __forceinline__ void gauss_chain(float x0, float eta, float dr, float
 // x^zeta for x >= 0 as x^n * x^f with n = floor(zeta): the integer power by
 // repeated squaring (a few roundings) and only the fractional power through
 // the SFU exp2/log2 approximations, whose log2 error is then scaled by f < 1
-// instead of by zeta (14.1).
+// instead of by zeta (14.1).  N >= 0 is n known at compile time (the kernels
+// built for the ANI-2x exponent): the same products in the same order, with
+// the bit tests and unused squarings gone; N < 0 reads n at run time.
+template <int N>
 __device__ __forceinline__ float zeta_pow(float x, int n, float f) {
   if (x <= 0.f) return 0.f;
   float r = 1.f, b = x;
 #pragma unroll
   for (int k = 0; k < 6; ++k) {  // n < 64
-    r = ((n >> k) & 1) ? r * b : r;
+    const bool bit = N >= 0 ? ((N >> k) & 1) != 0 : ((n >> k) & 1) != 0;
+    r = bit ? r * b : r;
+    if (N >= 0 && (N >> (k + 1)) == 0) break;
     b *= b;
   }
   return f != 0.f ? r * exp2f_approx_pos(f * __log2f(x)) : r;
 }
+
+// integer part of zeta - 1 for a compile-time integer part ZN of zeta
+__host__ __device__ constexpr int zn_minus1(int zn) { return zn >= 0 ? zn - 1 : -1; }
 
 // Warp-collective: stage row i.  Returns, in lanes s < S, the per-species
 // radial and angular counts and exclusive offsets.  Lanes holding the same
@@ -350,7 +358,7 @@ __device__ __forceinline__ void store_feature(int out_kind, void* out, void* out
   }
 }
 
-template <int RD, int AD, int AS>
+template <int RD, int AD, int AS, int ZN>
 __global__ void __launch_bounds__(kAevWarps * 32)
 k_aev_forward(const float4* __restrict__ xyzs, int n, const int* __restrict__ atom_sys,
               const float* __restrict__ sys_cell, const int* __restrict__ nbr_j,
@@ -436,7 +444,7 @@ k_aev_forward(const float4* __restrict__ xyzs, int n, const int* __restrict__ at
 #pragma unroll
           for (int z = 0; z < AS; ++z) {
             float cz = ct * K.cosz[z] + stt * K.sinz[z];
-            A[z] = f * zeta_pow(1.0f + cz, K.zeta_n, K.zeta_f);
+            A[z] = f * zeta_pow<ZN>(1.0f + cz, K.zeta_n, K.zeta_f);
           }
           const float dm = 0.5f * (ua.w + ub.w);
           gauss_chain<AD>(dm - K.shift_a[0], eta_a, K.dra, K.gc2a, B);
@@ -462,7 +470,7 @@ __host__ __device__ __forceinline__ size_t bwd_bytes(int S, int RD, int cap) {
   return (stage_bytes(cap, false) + (size_t)S * (RD + 1) * 4 + (2 * kMaxBlk + 2) * 4 + 15) / 16 * 16;
 }
 
-template <int RD, int AD, int AS, bool kVir>
+template <int RD, int AD, int AS, int ZN, bool kVir>
 __global__ void __launch_bounds__(kAevWarps * 32, 4)
 k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ atom_sys,
                const float* __restrict__ sys_cell, const int* __restrict__ nbr_j,
@@ -582,7 +590,7 @@ k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ a
       float cz = ct * K.cosz[z] + stt * K.sinz[z];
       float sz = stt * K.cosz[z] - ct * K.sinz[z];
       float bs = fmaxf(1.0f + cz, 0.f);
-      float pw1 = zeta_pow(bs, K.zeta1_n, K.zeta1_f);
+      float pw1 = zeta_pow<zn_minus1(ZN)>(bs, K.zeta1_n, K.zeta1_f);
       A[z] = pw1 * bs;
       Ap[z] = -zeta * pw1 * sz;
     }
@@ -595,11 +603,21 @@ k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ a
       const float x = dm - K.shift_a[r];
       const float Bv = Bs[r];
       float GA = 0.f, GAp = 0.f;
+      // the pair block (32 floats) starts 16-byte aligned when ld and S * RD
+      // are multiples of 4 (checked by the launcher)
+      float gz[AS];
+#pragma unroll
+      for (int z4 = 0; z4 < AS / 4; ++z4) {
+        const float4 q = __ldg(reinterpret_cast<const float4*>(gp + r * AS) + z4);
+        gz[4 * z4] = q.x;
+        gz[4 * z4 + 1] = q.y;
+        gz[4 * z4 + 2] = q.z;
+        gz[4 * z4 + 3] = q.w;
+      }
 #pragma unroll
       for (int z = 0; z < AS; ++z) {
-        const float gv = __ldg(gp + r * AS + z);
-        GA = fmaf(gv, A[z], GA);
-        GAp = fmaf(gv, Ap[z], GAp);
+        GA = fmaf(gz[z], A[z], GA);
+        GAp = fmaf(gz[z], Ap[z], GAp);
       }
       Q = fmaf(GA, Bv, Q);
       Th = fmaf(GAp, Bv, Th);
@@ -685,7 +703,7 @@ __host__ __device__ __forceinline__ size_t jvp_bytes(int cap) {
   return (stage_bytes(cap) + (size_t)cap * (4 + 16 + 8) + 15) / 16 * 16;
 }
 
-template <int RD, int AD, int AS>
+template <int RD, int AD, int AS, int ZN>
 __global__ void __launch_bounds__(kAevWarps * 32)
 k_aev_tangent(const float4* __restrict__ xyzs, int n, const int* __restrict__ atom_sys,
               const float* __restrict__ sys_cell, const int* __restrict__ nbr_j,
@@ -798,7 +816,7 @@ k_aev_tangent(const float4* __restrict__ xyzs, int n, const int* __restrict__ at
             const float cz = ct * K.cosz[z] + stt * K.sinz[z];
             const float dcz = dct * K.cosz[z] + dstt * K.sinz[z];
             const float bs = fmaxf(1.0f + cz, 0.f);
-            const float pw1 = zeta_pow(bs, K.zeta1_n, K.zeta1_f);  // (1 + cz)^(zeta - 1)
+            const float pw1 = zeta_pow<zn_minus1(ZN)>(bs, K.zeta1_n, K.zeta1_f);  // (1 + cz)^(zeta - 1)
             A[z] = f * pw1 * bs;
             dA[z] = df * pw1 * bs + f * zeta * pw1 * dcz;
           }
@@ -831,29 +849,32 @@ __global__ void k_pack(const float* __restrict__ coords, const int* __restrict__
   xyzs[i] = make_float4(coords[3 * i], coords[3 * i + 1], coords[3 * i + 2], __int_as_float(sp[i]));
 }
 
-template <int RD, int AD, int AS>
+template <int RD, int AD, int AS, int ZN>
 struct AevKernels {
-  static constexpr auto fwd = k_aev_forward<RD, AD, AS>;
-  static constexpr auto bwd = k_aev_backward<RD, AD, AS, false>;
-  static constexpr auto bwdv = k_aev_backward<RD, AD, AS, true>;
-  static constexpr auto tan = k_aev_tangent<RD, AD, AS>;
+  static constexpr auto fwd = k_aev_forward<RD, AD, AS, ZN>;
+  static constexpr auto bwd = k_aev_backward<RD, AD, AS, ZN, false>;
+  static constexpr auto bwdv = k_aev_backward<RD, AD, AS, ZN, true>;
+  static constexpr auto tan = k_aev_tangent<RD, AD, AS, ZN>;
 };
 
-// (RD, AD, AS) combinations compiled: radial 16/32 x angular (8,4) / (4,8).
+// (RD, AD, AS) combinations compiled: radial 16/32 x angular (8,4) / (4,8),
+// with the integer part of zeta read at run time; the ANI-2x layout
+// (16, 4, 8) with zeta in [14, 15) also has kernels with it built in.
 template <typename Fn>
 bool dispatch(const AevConst& K, Fn&& fn) {
-  if (K.RD == 16 && K.AD == 8 && K.AS == 4) return fn(AevKernels<16, 8, 4>{});
-  if (K.RD == 16 && K.AD == 4 && K.AS == 8) return fn(AevKernels<16, 4, 8>{});
-  if (K.RD == 32 && K.AD == 8 && K.AS == 4) return fn(AevKernels<32, 8, 4>{});
-  if (K.RD == 32 && K.AD == 4 && K.AS == 8) return fn(AevKernels<32, 4, 8>{});
+  if (K.RD == 16 && K.AD == 4 && K.AS == 8 && K.zeta_n == 14) return fn(AevKernels<16, 4, 8, 14>{});
+  if (K.RD == 16 && K.AD == 8 && K.AS == 4) return fn(AevKernels<16, 8, 4, -1>{});
+  if (K.RD == 16 && K.AD == 4 && K.AS == 8) return fn(AevKernels<16, 4, 8, -1>{});
+  if (K.RD == 32 && K.AD == 8 && K.AS == 4) return fn(AevKernels<32, 8, 4, -1>{});
+  if (K.RD == 32 && K.AD == 4 && K.AS == 8) return fn(AevKernels<32, 4, 8, -1>{});
   return false;
 }
 
 // Opt a kernel in to the largest dynamic shared memory it can use, once.
 size_t set_smem(const void* fn, size_t bytes) {
-  static const void* done[16] = {};
+  static const void* done[32] = {};
   if (bytes > 48 * 1024) {
-    for (int k = 0; k < 16; ++k) {
+    for (int k = 0; k < 32; ++k) {
       if (done[k] == fn) return bytes;
       if (!done[k]) {
         if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess)
@@ -924,6 +945,8 @@ static int aev_backward_launch(const float* xyzs, int natoms, const int* atom_sy
   if (natoms == 0) return FENNOL_OK;
   if (!xyzs || !atom_sys || !nbr_j || !nbr_shift || !nbr_count || !atom_row || !daev || !forces4)
     return FENNOL_ERR_INVALID;
+  // the kernel reads dE/dAEV pair blocks as float4
+  if ((ld & 3) != 0 || ((uintptr_t)daev & 15) != 0) return FENNOL_ERR_INVALID;
   size_t bytes = (size_t)kAevWarps * bwd_bytes(K.S, K.RD, capacity);
   if (bytes > 200 * 1024) return FENNOL_ERR_UNSUPPORTED;
   int blocks = (natoms + kAevWarps - 1) / kAevWarps;

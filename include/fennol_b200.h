@@ -206,6 +206,8 @@ int fennol_aev_forward(const float* xyzs, int natoms, const int* atom_sys, const
  * (x, y, z, unused).  Replaces the reverse-mode transpose of the AEV
  * (jax.grad through ani.py and the graph processors, fennix.py:260-272).
  * forces4 must be zeroed (or hold other force terms) before the call.
+ * daev must be 16-byte aligned and ld a multiple of 4 (FENNOL_ERR_INVALID
+ * otherwise).
  */
 int fennol_aev_backward(const float* xyzs, int natoms, const int* atom_sys,
                         const float* sys_cell, const int* nbr_j, const unsigned* nbr_shift,
