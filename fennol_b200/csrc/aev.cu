@@ -333,6 +333,22 @@ __device__ __forceinline__ void diag_ab(int t, int n, int& a, int& b) {
   b = a + u + 1;
 }
 
+// q = floor(v / n), r = v - q n for 0 <= v < 2^16 and 1 <= n <= 256, from a
+// float reciprocal rn = 1/n: (v + 1/2) / n lies at least 1/(2n) from an
+// integer, far more than the float error of (v + 1/2) * rn; the correction
+// step keeps the result exact even so.
+__device__ __forceinline__ void div_small(int v, int n, float rn, int& q, int& r) {
+  q = (int)(((float)v + 0.5f) * rn);
+  r = v - q * n;
+  if (r < 0) {
+    --q;
+    r += n;
+  } else if (r >= n) {
+    ++q;
+    r -= n;
+  }
+}
+
 // Reduce v[32] over the warp so that lane f returns sum over lanes of v[f].
 __device__ __forceinline__ float transpose_reduce32(float* v, int lane) {
 #pragma unroll
@@ -467,7 +483,7 @@ k_aev_forward(const float4* __restrict__ xyzs, int n, const int* __restrict__ at
 constexpr int kMaxBlk = kMaxP;  // species-pair blocks of one centre atom
 
 __host__ __device__ __forceinline__ size_t bwd_bytes(int S, int RD, int cap) {
-  return (stage_bytes(cap, false) + (size_t)S * (RD + 1) * 4 + (2 * kMaxBlk + 2) * 4 + 15) / 16 * 16;
+  return (stage_bytes(cap, false) + (size_t)S * (RD + 1) * 4 + (6 * kMaxBlk + 2) * 4 + 15) / 16 * 16;
 }
 
 template <int RD, int AD, int AS, int ZN, bool kVir>
@@ -534,8 +550,14 @@ k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ a
   // into consecutive warp rounds (lane per triplet); each lane reads the
   // dE/dAEV row of its own pair block.
   const float zeta = K.zeta, c_ang = K.c_ang, eta_a = K.eta_a;
-  int* blk_cum = blkw;               // [kMaxBlk + 2]: first triplet of each block, end, count
-  int* blk_ss = blkw + kMaxBlk + 2;  // [kMaxBlk] s1 | s2 << 8
+  // Block table, built once per centre so that a triplet needs no per-species
+  // lookups: first triplet, sizes, offsets, pair index, 1/n of each block.
+  int* blk_cum = blkw;                                   // [kMaxBlk + 2]: first triplet, end, count
+  int* blk_n = blkw + kMaxBlk + 2;                       // n1 | n2 << 8 | (s1 == s2) << 16
+  int* blk_o = blk_n + kMaxBlk;                          // o1 | o2 << 8
+  int* blk_p = blk_o + kMaxBlk;                          // species-pair index
+  float* blk_r1 = reinterpret_cast<float*>(blk_p + kMaxBlk);  // 1 / n1
+  float* blk_r2 = blk_r1 + kMaxBlk;                           // 1 / n2
   if (lane == 0) {
     int nb = 0, tot = 0;
     for (int s1 = 0; s1 < S; ++s1) {
@@ -549,7 +571,11 @@ k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ a
         if (o1 + n1 > kCapA || o2 + n2 > kCapA) T = 0;
         if (T == 0) continue;
         blk_cum[nb] = tot;
-        blk_ss[nb] = s1 | (s2 << 8);
+        blk_n[nb] = n1 | (n2 << 8) | ((s1 == s2) << 16);
+        blk_o[nb] = o1 | (o2 << 8);
+        blk_p[nb] = triu_pair(s1, s2, S);
+        blk_r1[nb] = 1.0f / (float)n1;
+        blk_r2[nb] = 1.0f / (float)n2;
         tot += T;
         ++nb;
       }
@@ -563,21 +589,26 @@ k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ a
   for (int t = lane; t < Ttot; t += 32) {
     int k = 0;
     while (k + 1 < nblk && blk_cum[k + 1] <= t) ++k;
-    const int s1 = blk_ss[k] & 0xFF, s2 = blk_ss[k] >> 8;
     const int tl = t - blk_cum[k];
-    const int n1 = min(st.cntw[S + s1], kCapA), n2 = min(st.cntw[S + s2], kCapA);
-    const int o1 = st.cntw[3 * S + s1] - st.cntw[S + s1], o2 = st.cntw[3 * S + s2] - st.cntw[S + s2];
+    const int nn = blk_n[k], oo = blk_o[k];
+    const int n1 = nn & 0xFF, n2 = (nn >> 8) & 0xFF;
+    const int o1 = oo & 0xFF, o2 = oo >> 8;
     int a, b;
-    if (s1 == s2) {
+    if (nn >> 16) {
       diag_ab(tl, n1, a, b);
       a += o1;
       b += o1;
     } else {
-      const int aa = tl % n1, dd = tl / n1;
+      // aa = tl mod n1, dd = tl div n1, b = o2 + (aa + dd) mod n2, as exact
+      // quotients through 1/n (n <= 96, tl < 96 * 96)
+      int dd, aa, bb;
+      div_small(tl, n1, blk_r1[k], dd, aa);
+      int q2;
+      div_small(aa + dd, n2, blk_r2[k], q2, bb);
       a = o1 + aa;
-      b = o2 + (aa + dd) % n2;
+      b = o2 + bb;
     }
-    const int p = triu_pair(s1, s2, S);
+    const int p = blk_p[k];
     const float* gp = g + FR + p * 32;
     const float4 ua = st.au[a], ub = st.au[b];
     const float2 fa2 = st.af[a], fb2 = st.af[b];
@@ -859,10 +890,11 @@ struct AevKernels {
 
 // (RD, AD, AS) combinations compiled: radial 16/32 x angular (8,4) / (4,8),
 // with the integer part of zeta read at run time; the ANI-2x layout
-// (16, 4, 8) with zeta in [14, 15) also has kernels with it built in.
+// (16 radial shifts, 8 angular shifts x 4 sections) with zeta in [14, 15)
+// also has kernels with it built in.
 template <typename Fn>
 bool dispatch(const AevConst& K, Fn&& fn) {
-  if (K.RD == 16 && K.AD == 4 && K.AS == 8 && K.zeta_n == 14) return fn(AevKernels<16, 4, 8, 14>{});
+  if (K.RD == 16 && K.AD == 8 && K.AS == 4 && K.zeta_n == 14) return fn(AevKernels<16, 8, 4, 14>{});
   if (K.RD == 16 && K.AD == 8 && K.AS == 4) return fn(AevKernels<16, 8, 4, -1>{});
   if (K.RD == 16 && K.AD == 4 && K.AS == 8) return fn(AevKernels<16, 4, 8, -1>{});
   if (K.RD == 32 && K.AD == 8 && K.AS == 4) return fn(AevKernels<32, 8, 4, -1>{});
