@@ -227,15 +227,18 @@ def kernel_times(pot, eng, reps=20):
     st = torch.cuda.current_stream().cuda_stream
     lp = C_ptr(pot.params)
 
+    # the staged pair, as the MD step launches it
     def aev_fwd():
-        call("fennol_aev_forward", ws.xyzs.data_ptr(), lay.n, lay.t_atom_sys.data_ptr(), lay.t_cell.data_ptr(),
-             g.rad_j.data_ptr(), g.rad_s.data_ptr(), g.rad_n.data_ptr(), g.cap_r, lp, lay.t_atom_row.data_ptr(),
-             ws.aev_kind, ws.x.data_ptr(), _ptr(ws.x_lo), ws.x.shape[1], ws.status.data_ptr(), st)
+        call("fennol_aev_forward_staged", ws.xyzs.data_ptr(), lay.n, lay.t_atom_sys.data_ptr(),
+             lay.t_cell.data_ptr(), g.rad_j.data_ptr(), g.rad_s.data_ptr(), g.rad_n.data_ptr(), g.cap_r, lp,
+             lay.t_atom_row.data_ptr(), ws.aev_kind, ws.x.data_ptr(), _ptr(ws.x_lo), ws.x.shape[1],
+             g.aev_stage.data_ptr(), g.aev_stage.numel(), ws.status.data_ptr(), st)
 
     def aev_bwd():
-        call("fennol_aev_backward", ws.xyzs.data_ptr(), lay.n, lay.t_atom_sys.data_ptr(), lay.t_cell.data_ptr(),
-             g.rad_j.data_ptr(), g.rad_s.data_ptr(), g.rad_n.data_ptr(), g.cap_r, lp, lay.t_atom_row.data_ptr(),
-             ws.dx.data_ptr(), ws.dx.shape[1], ws.forces4.data_ptr(), ws.status.data_ptr(), st)
+        call("fennol_aev_backward_staged", ws.xyzs.data_ptr(), lay.n, lay.t_atom_sys.data_ptr(),
+             lay.t_cell.data_ptr(), g.rad_j.data_ptr(), g.rad_s.data_ptr(), g.rad_n.data_ptr(), g.cap_r, lp,
+             lay.t_atom_row.data_ptr(), ws.dx.data_ptr(), ws.dx.shape[1], ws.forces4.data_ptr(),
+             g.aev_stage.data_ptr(), ws.status.data_ptr(), st)
 
     out = {"aev_forward": time_launch(aev_fwd, reps), "mlp": time_mlp(pot, eng, reps),
            "aev_backward": time_launch(aev_bwd, reps)}

@@ -86,6 +86,9 @@ _SIGNATURES = {
     "fennol_aev_forward": (I, [P, I, P, P, P, P, P, I, C.POINTER(AEVParams), P, I, P, P, I, P, P]),
     "fennol_aev_backward": (I, [P, I, P, P, P, P, P, I, C.POINTER(AEVParams), P, P, I, P, P, P]),
     "fennol_aev_backward_virial": (I, [P, I, P, P, P, P, P, I, C.POINTER(AEVParams), P, P, I, P, P, P, P]),
+    "fennol_aev_stage_bytes": (SZ, [I, I]),
+    "fennol_aev_forward_staged": (I, [P, I, P, P, P, P, P, I, C.POINTER(AEVParams), P, I, P, P, I, P, SZ, P, P]),
+    "fennol_aev_backward_staged": (I, [P, I, P, P, P, P, P, I, C.POINTER(AEVParams), P, P, I, P, P, P, P]),
     "fennol_virial_reduce": (I, [P, I, P, I, D, P, P]),
     "fennol_aev_tangent": (I, [P, I, P, P, P, P, P, I, C.POINTER(AEVParams), P, P, P, I, P, P]),
     "fennol_mlp_workspace_bytes": (SZ, [I, I, I, C.POINTER(MLPWeights)]),

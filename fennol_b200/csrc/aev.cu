@@ -37,6 +37,7 @@ struct AevConst {
   int zeta1_n;                      // the same split of zeta - 1
   float zeta1_f;
   float dra, gc2a;                  // angular shift spacing, exp(-2 eta_a dra^2)
+  float drr, gc2r, inv_drr, lim_r;  // radial: spacing, exp(-2 eta_r drr^2), 1 / drr, sqrt(80 / eta_r)
   float shift_r[32];
   float shift_a[32];
   float cosz[32], sinz[32];
@@ -79,6 +80,11 @@ bool make_const(const fennol_aev_params* p, AevConst* k) {
     const double dra = (p->angular_cutoff - p->angular_start) / AD;
     k->dra = (float)dra;
     k->gc2a = (float)std::exp(-2.0 * (double)p->angular_eta * dra * dra);
+    const double drr = (p->radial_cutoff - p->radial_start) / RD;
+    k->drr = (float)drr;
+    k->gc2r = (float)std::exp(-2.0 * (double)p->radial_eta * drr * drr);
+    k->inv_drr = (float)(1.0 / drr);
+    k->lim_r = (float)std::sqrt(80.0 / (double)p->radial_eta);
   }
   for (int r = 0; r < 32; ++r) {
     k->shift_r[r] = r < RD ? (float)(p->radial_start + (p->radial_cutoff - p->radial_start) * r / RD) : 0.f;
@@ -188,6 +194,33 @@ __device__ __forceinline__ void gauss_chain(float x0, float eta, float dr, float
     B[r] = b;
     b *= g;
     g *= c2;
+  }
+}
+
+// The same for shifts spread over a wider range (the radial ones), where the
+// first term underflows for most distances: B[r] = exp(-eta (x0 - r dr)^2),
+// r < N, from two exponentials.  Terms below exp(-80) (< 2e-35, far below anything a
+// float32 sum of the others registers) are 0; from the first shift r0 at or
+// above that bound the chain B[r+1] = B[r] g[r], g[r] = exp(eta dr (2 (x0 -
+// r dr) - dr)), g[r+1] = g[r] c2 with c2 = exp(-2 eta dr^2) takes over.  B
+// rises to at most 1 and then falls, and g stays below exp(2 eta dr (lim +
+// dr)), so nothing overflows.  lim = sqrt(80 / eta), inv_dr = 1 / dr.
+template <int N>
+__device__ __forceinline__ void gauss_chain_from(float x0, float eta, float dr, float inv_dr, float c2, float lim,
+                                                 float* B) {
+  const float rs = ceilf((x0 - lim) * inv_dr);
+  const int r0 = rs <= 0.f ? 0 : (rs >= (float)N ? N : (int)rs);
+  const float xs = x0 - (float)r0 * dr;
+  float b = fexp(-eta * xs * xs);
+  float g = fexp(eta * dr * (2.f * xs - dr));
+#pragma unroll
+  for (int r = 0; r < N; ++r) {
+    const bool on = r >= r0;
+    B[r] = on ? b : 0.f;
+    if (on) {
+      b *= g;
+      g *= c2;
+    }
   }
 }
 
@@ -374,13 +407,45 @@ __device__ __forceinline__ void store_feature(int out_kind, void* out, void* out
   }
 }
 
+// Warp-collective copy of one centre's staged neighbourhood into the shared
+// Stage view `dst` (carved at dst_base) from a global record of the same
+// layout (carve_stage(.., cap, false)) at src_base: the cnt unsorted edges
+// (vector, d^2, key), the na angular entries (unit vector and d, fc and dfc,
+// row slot) and the 4 S counters.  The forward saves the record for the
+// adjoint of the same step, which then skips the gathers and the sort.
+// Every global address is formed from src_base plus the array's offset in
+// the layout (a difference of two shared pointers): a pointer computed from
+// a shared one would be taken as a shared-window address.
+template <typename T>
+__device__ __forceinline__ const T* in_record(const char* src_base, const char* dst_base, const T* p) {
+  return reinterpret_cast<const T*>(src_base + (reinterpret_cast<const char*>(p) - dst_base));
+}
+__device__ __forceinline__ void copy_stage(const Stage& dst, const char* dst_base, const char* src_base, int cnt,
+                                           int na, int S, int lane) {
+  const float4* tmp = in_record(src_base, dst_base, dst.tmp);
+  const int* tkey = in_record(src_base, dst_base, dst.tkey);
+  for (int k = lane; k < cnt; k += 32) {
+    dst.tmp[k] = tmp[k];
+    dst.tkey[k] = tkey[k];
+  }
+  const float4* au = in_record(src_base, dst_base, dst.au);
+  const float2* af = in_record(src_base, dst_base, dst.af);
+  const int* aslot = in_record(src_base, dst_base, dst.aslot);
+  for (int k = lane; k < na; k += 32) {
+    dst.au[k] = au[k];
+    dst.af[k] = af[k];
+    dst.aslot[k] = aslot[k];
+  }
+  if (lane < 4 * S) dst.cntw[lane] = in_record(src_base, dst_base, dst.cntw)[lane];
+}
+
 template <int RD, int AD, int AS, int ZN>
 __global__ void __launch_bounds__(kAevWarps * 32)
 k_aev_forward(const float4* __restrict__ xyzs, int n, const int* __restrict__ atom_sys,
               const float* __restrict__ sys_cell, const int* __restrict__ nbr_j,
               const unsigned* __restrict__ nbr_shift, const int* __restrict__ nbr_count, int cap,
               const AevConst K, const int* __restrict__ atom_row, int out_kind, void* __restrict__ out,
-              void* __restrict__ out_lo, int ld, int* status) {
+              void* __restrict__ out_lo, int ld, int* status, char* __restrict__ stage_g) {
   pdl_wait();
   extern __shared__ __align__(16) char smem_c[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -394,11 +459,27 @@ k_aev_forward(const float4* __restrict__ xyzs, int n, const int* __restrict__ at
   int cnt = nbr_count[i];
   if (cnt > cap) cnt = cap;
   int cnt_r, off_r, cnt_a, off_a, na;
-  stage_row<false>(st, st.cntw, xyzs, pi, c, nbr_j, nbr_shift, (size_t)i * cap, cnt, K, lane, cnt_r, off_r, cnt_a,
-                   off_a, na);
+  stage_row<true>(st, st.cntw, xyzs, pi, c, nbr_j, nbr_shift, (size_t)i * cap, cnt, K, lane, cnt_r, off_r, cnt_a,
+                  off_a, na);
   if (lane == 0) {
     status_max(status, ST_ANG_MAXCOUNT, na);
     if (na > kCapA) status_set(status, ST_ANG_OVERFLOW);
+  }
+  if (stage_g) {
+    // the saved record uses the adjoint's layout (no sorted radial entries)
+    char* rec = stage_g + (size_t)i * stage_bytes(cap, false);
+    const Stage rs = carve_stage(rec, cap, false);
+    const int nac = min(na, kCapA);
+    for (int k = lane; k < cnt; k += 32) {
+      rs.tmp[k] = st.tmp[k];
+      rs.tkey[k] = st.tkey[k];
+    }
+    for (int k = lane; k < nac; k += 32) {
+      rs.au[k] = st.au[k];
+      rs.af[k] = st.af[k];
+      rs.aslot[k] = st.aslot[k];
+    }
+    if (lane < 4 * S) rs.cntw[lane] = st.cntw[lane];
   }
   const size_t orow = (size_t)atom_row[i] * ld;
 
@@ -486,13 +567,14 @@ __host__ __device__ __forceinline__ size_t bwd_bytes(int S, int RD, int cap) {
   return (stage_bytes(cap, false) + (size_t)S * (RD + 1) * 4 + (6 * kMaxBlk + 2) * 4 + 15) / 16 * 16;
 }
 
-template <int RD, int AD, int AS, int ZN, bool kVir>
+template <int RD, int AD, int AS, int ZN, bool kVir, bool kStaged>
 __global__ void __launch_bounds__(kAevWarps * 32, 4)
 k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ atom_sys,
                const float* __restrict__ sys_cell, const int* __restrict__ nbr_j,
                const unsigned* __restrict__ nbr_shift, const int* __restrict__ nbr_count, int cap,
                const AevConst K, const int* __restrict__ atom_row, const float* __restrict__ daev,
-               int ld, float4* __restrict__ forces, float* __restrict__ atom_virial, int* status) {
+               int ld, float4* __restrict__ forces, float* __restrict__ atom_virial, int* status,
+               const char* __restrict__ stage_g) {
   pdl_wait();
   extern __shared__ __align__(16) char smem_c[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -516,10 +598,20 @@ k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ a
   int cnt = nbr_count[i];
   if (cnt > cap) cnt = cap;
   const size_t row = (size_t)i * cap;
-  int cnt_r, off_r, cnt_a, off_a, na;
-  stage_row<true, false, false>(st, st.cntw, xyzs, pi, c, nbr_j, nbr_shift, row, cnt, K, lane, cnt_r, off_r,
-                                cnt_a, off_a, na);
-  if (na > kCapA && lane == 0) status_set(status, ST_ANG_OVERFLOW);
+  if constexpr (kStaged) {
+    // the forward of this step staged this centre already
+    const char* rec = stage_g + (size_t)i * stage_bytes(cap, false);
+    const int* cw = in_record(rec, base, st.cntw);
+    int na = 0;
+    for (int s2 = 0; s2 < S; ++s2) na += cw[S + s2];
+    copy_stage(st, base, rec, cnt, min(na, kCapA), S, lane);
+    __syncwarp();
+  } else {
+    int cnt_r, off_r, cnt_a, off_a, na;
+    stage_row<true, false, false>(st, st.cntw, xyzs, pi, c, nbr_j, nbr_shift, row, cnt, K, lane, cnt_r, off_r,
+                                  cnt_a, off_a, na);
+    if (na > kCapA && lane == 0) status_set(status, ST_ANG_OVERFLOW);
+  }
 
   // ---- radial: lane per neighbour (row order), gradient into gk[4k..4k+2]
   for (int k = lane; k < cnt; k += 32) {
@@ -535,11 +627,12 @@ k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ a
     }
     const float* grow = gr + sj * (RD + 1);
     float dEdd = 0.f;
-#pragma unroll 8
+    float Br[RD];
+    gauss_chain_from<RD>(d - K.shift_r[0], K.eta_r, K.drr, K.inv_drr, K.gc2r, K.lim_r, Br);
+#pragma unroll
     for (int r = 0; r < RD; ++r) {
       float x = d - K.shift_r[r];
-      float e = fexp(-K.eta_r * x * x);
-      dEdd = fmaf(grow[r] * e, dfc - 2.f * K.eta_r * x * fc, dEdd);
+      dEdd = fmaf(grow[r] * Br[r], dfc - 2.f * K.eta_r * x * fc, dEdd);
     }
     float sc = v.w > 1e-5f ? 0.25f * dEdd / d : 0.f;
     st.tmp[k] = make_float4(sc * v.x, sc * v.y, sc * v.z, 0.f);
@@ -883,8 +976,9 @@ __global__ void k_pack(const float* __restrict__ coords, const int* __restrict__
 template <int RD, int AD, int AS, int ZN>
 struct AevKernels {
   static constexpr auto fwd = k_aev_forward<RD, AD, AS, ZN>;
-  static constexpr auto bwd = k_aev_backward<RD, AD, AS, ZN, false>;
-  static constexpr auto bwdv = k_aev_backward<RD, AD, AS, ZN, true>;
+  static constexpr auto bwd = k_aev_backward<RD, AD, AS, ZN, false, false>;
+  static constexpr auto bwdv = k_aev_backward<RD, AD, AS, ZN, true, false>;
+  static constexpr auto bwds = k_aev_backward<RD, AD, AS, ZN, false, true>;
   static constexpr auto tan = k_aev_tangent<RD, AD, AS, ZN>;
 };
 
@@ -938,11 +1032,10 @@ extern "C" int fennol_pack_atoms(const float* coords, const int* species_idx, in
   return FENNOL_OK;
 }
 
-extern "C" int fennol_aev_forward(const float* xyzs, int natoms, const int* atom_sys,
-                                  const float* sys_cell, const int* nbr_j, const unsigned* nbr_shift,
-                                  const int* nbr_count, int capacity, const fennol_aev_params* p,
-                                  const int* atom_row, int out_kind, void* out, void* out_lo, int ld,
-                                  int* status, void* stream) {
+static int aev_forward_launch(const float* xyzs, int natoms, const int* atom_sys, const float* sys_cell,
+                              const int* nbr_j, const unsigned* nbr_shift, const int* nbr_count, int capacity,
+                              const fennol_aev_params* p, const int* atom_row, int out_kind, void* out,
+                              void* out_lo, int ld, int* status, void* stage, void* stream) {
   AevConst K;
   if (!make_const(p, &K)) return FENNOL_ERR_UNSUPPORTED;
   if (natoms < 0 || capacity <= 0 || ld < K.F) return FENNOL_ERR_INVALID;
@@ -959,7 +1052,7 @@ extern "C" int fennol_aev_forward(const float* xyzs, int natoms, const int* atom
     if (!smem) return false;
     if (launch_pdl(ks.fwd, blocks, kAevWarps * 32, smem, (cudaStream_t)stream, 
         (const float4*)xyzs, natoms, atom_sys, sys_cell, nbr_j, nbr_shift, nbr_count, capacity, K,
-        atom_row, out_kind, out, out_lo, ld, status) != cudaSuccess) return false;
+        atom_row, out_kind, out, out_lo, ld, status, (char*)stage) != cudaSuccess) return false;
     return true;
   });
   if (!launched) return FENNOL_ERR_UNSUPPORTED;
@@ -967,10 +1060,36 @@ extern "C" int fennol_aev_forward(const float* xyzs, int natoms, const int* atom
   return FENNOL_OK;
 }
 
+extern "C" int fennol_aev_forward(const float* xyzs, int natoms, const int* atom_sys,
+                                  const float* sys_cell, const int* nbr_j, const unsigned* nbr_shift,
+                                  const int* nbr_count, int capacity, const fennol_aev_params* p,
+                                  const int* atom_row, int out_kind, void* out, void* out_lo, int ld,
+                                  int* status, void* stream) {
+  return aev_forward_launch(xyzs, natoms, atom_sys, sys_cell, nbr_j, nbr_shift, nbr_count, capacity, p, atom_row,
+                            out_kind, out, out_lo, ld, status, nullptr, stream);
+}
+
+extern "C" size_t fennol_aev_stage_bytes(int natoms, int capacity) {
+  if (natoms < 0 || capacity <= 0) return 0;
+  return (size_t)natoms * stage_bytes(capacity, false);
+}
+
+extern "C" int fennol_aev_forward_staged(const float* xyzs, int natoms, const int* atom_sys,
+                                         const float* sys_cell, const int* nbr_j, const unsigned* nbr_shift,
+                                         const int* nbr_count, int capacity, const fennol_aev_params* p,
+                                         const int* atom_row, int out_kind, void* out, void* out_lo, int ld,
+                                         void* stage, size_t stage_bytes_, int* status, void* stream) {
+  if (natoms > 0 && (!stage || ((uintptr_t)stage & 15) != 0)) return FENNOL_ERR_INVALID;
+  if (stage_bytes_ < fennol_aev_stage_bytes(natoms, capacity)) return FENNOL_ERR_WORKSPACE;
+  return aev_forward_launch(xyzs, natoms, atom_sys, sys_cell, nbr_j, nbr_shift, nbr_count, capacity, p, atom_row,
+                            out_kind, out, out_lo, ld, status, stage, stream);
+}
+
 static int aev_backward_launch(const float* xyzs, int natoms, const int* atom_sys, const float* sys_cell,
                                const int* nbr_j, const unsigned* nbr_shift, const int* nbr_count, int capacity,
                                const fennol_aev_params* p, const int* atom_row, const float* daev, int ld,
-                               float* forces4, float* atom_virial, int* status, void* stream) {
+                               float* forces4, float* atom_virial, int* status, const void* stage,
+                               void* stream) {
   AevConst K;
   if (!make_const(p, &K)) return FENNOL_ERR_UNSUPPORTED;
   if (natoms < 0 || capacity <= 0 || ld < K.F) return FENNOL_ERR_INVALID;
@@ -983,12 +1102,12 @@ static int aev_backward_launch(const float* xyzs, int natoms, const int* atom_sy
   if (bytes > 200 * 1024) return FENNOL_ERR_UNSUPPORTED;
   int blocks = (natoms + kAevWarps - 1) / kAevWarps;
   bool launched = dispatch(K, [&](auto ks) {
-    auto fn = atom_virial ? ks.bwdv : ks.bwd;
+    auto fn = atom_virial ? ks.bwdv : (stage ? ks.bwds : ks.bwd);
     size_t smem = set_smem((const void*)fn, bytes);
     if (!smem) return false;
     if (launch_pdl(fn, blocks, kAevWarps * 32, smem, (cudaStream_t)stream, 
         (const float4*)xyzs, natoms, atom_sys, sys_cell, nbr_j, nbr_shift, nbr_count, capacity, K,
-        atom_row, daev, ld, (float4*)forces4, atom_virial, status) != cudaSuccess) return false;
+        atom_row, daev, ld, (float4*)forces4, atom_virial, status, (const char*)stage) != cudaSuccess) return false;
     return true;
   });
   if (!launched) return FENNOL_ERR_UNSUPPORTED;
@@ -1002,7 +1121,17 @@ extern "C" int fennol_aev_backward(const float* xyzs, int natoms, const int* ato
                                    const int* atom_row, const float* daev, int ld, float* forces4,
                                    int* status, void* stream) {
   return aev_backward_launch(xyzs, natoms, atom_sys, sys_cell, nbr_j, nbr_shift, nbr_count, capacity, p,
-                             atom_row, daev, ld, forces4, nullptr, status, stream);
+                             atom_row, daev, ld, forces4, nullptr, status, nullptr, stream);
+}
+
+extern "C" int fennol_aev_backward_staged(const float* xyzs, int natoms, const int* atom_sys,
+                                          const float* sys_cell, const int* nbr_j, const unsigned* nbr_shift,
+                                          const int* nbr_count, int capacity, const fennol_aev_params* p,
+                                          const int* atom_row, const float* daev, int ld, float* forces4,
+                                          const void* stage, int* status, void* stream) {
+  if (natoms > 0 && (!stage || ((uintptr_t)stage & 15) != 0)) return FENNOL_ERR_INVALID;
+  return aev_backward_launch(xyzs, natoms, atom_sys, sys_cell, nbr_j, nbr_shift, nbr_count, capacity, p,
+                             atom_row, daev, ld, forces4, nullptr, status, stage, stream);
 }
 
 extern "C" int fennol_aev_backward_virial(const float* xyzs, int natoms, const int* atom_sys,
@@ -1012,7 +1141,7 @@ extern "C" int fennol_aev_backward_virial(const float* xyzs, int natoms, const i
                                           float* atom_virial, int* status, void* stream) {
   if (natoms > 0 && !atom_virial) return FENNOL_ERR_INVALID;
   return aev_backward_launch(xyzs, natoms, atom_sys, sys_cell, nbr_j, nbr_shift, nbr_count, capacity, p,
-                             atom_row, daev, ld, forces4, atom_virial, status, stream);
+                             atom_row, daev, ld, forces4, atom_virial, status, nullptr, stream);
 }
 
 extern "C" int fennol_aev_tangent(const float* xyzs, int natoms, const int* atom_sys,

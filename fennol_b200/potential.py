@@ -271,6 +271,9 @@ class GraphBuffers:
         else:
             self.cap_r = cap
             self.rad_j, self.rad_s, self.rad_n = self.nbr_j, self.nbr_s, self.nbr_n
+        # per-centre staging that the AEV forward saves for the adjoint of the same step
+        sb = _lib.load().fennol_aev_stage_bytes(n, self.cap_r)
+        self.aev_stage = torch.empty(int(sb), dtype=torch.uint8, device=dev)
 
     def build(self, layout: BatchLayout, coords: torch.Tensor, status: torch.Tensor, stream: int,
               enable_flag: Optional[torch.Tensor] = None):
@@ -429,10 +432,18 @@ class ANIPotential:
         """AEV -> MLP -> energies (and adjoint -> forces) from the current radial list."""
         lib_p = C_ptr(self.params)
         n = layout.n
-        call("fennol_aev_forward", ws.xyzs.data_ptr(), n, layout.t_atom_sys.data_ptr(),
-             layout.t_cell.data_ptr(), g.rad_j.data_ptr(), g.rad_s.data_ptr(), g.rad_n.data_ptr(),
-             g.cap_r, lib_p, layout.t_atom_row.data_ptr(), ws.aev_kind, ws.x.data_ptr(),
-             _ptr(ws.x_lo), ws.x.shape[1], ws.status.data_ptr(), stream)
+        staged = want_forces and not want_virial  # the adjoint reuses the forward's staging
+        if staged:
+            call("fennol_aev_forward_staged", ws.xyzs.data_ptr(), n, layout.t_atom_sys.data_ptr(),
+                 layout.t_cell.data_ptr(), g.rad_j.data_ptr(), g.rad_s.data_ptr(), g.rad_n.data_ptr(),
+                 g.cap_r, lib_p, layout.t_atom_row.data_ptr(), ws.aev_kind, ws.x.data_ptr(),
+                 _ptr(ws.x_lo), ws.x.shape[1], g.aev_stage.data_ptr(), g.aev_stage.numel(),
+                 ws.status.data_ptr(), stream)
+        else:
+            call("fennol_aev_forward", ws.xyzs.data_ptr(), n, layout.t_atom_sys.data_ptr(),
+                 layout.t_cell.data_ptr(), g.rad_j.data_ptr(), g.rad_s.data_ptr(), g.rad_n.data_ptr(),
+                 g.cap_r, lib_p, layout.t_atom_row.data_ptr(), ws.aev_kind, ws.x.data_ptr(),
+                 _ptr(ws.x_lo), ws.x.shape[1], ws.status.data_ptr(), stream)
         call("fennol_mlp_energy_grad", self.precision, layout.rows, layout.ntiles,
              layout.t_tile_species.data_ptr(), layout.t_tile_row.data_ptr(), C_ptr(self.mlp.struct),
              ws.x.data_ptr(), _ptr(ws.x_lo), ws.e_rows.data_ptr(), ws.dx.data_ptr(),
@@ -451,10 +462,10 @@ class ANIPotential:
                  float(self.unit_scale), vir.data_ptr(), stream)
         elif want_forces:
             ws.forces4.zero_()
-            call("fennol_aev_backward", ws.xyzs.data_ptr(), n, layout.t_atom_sys.data_ptr(),
+            call("fennol_aev_backward_staged", ws.xyzs.data_ptr(), n, layout.t_atom_sys.data_ptr(),
                  layout.t_cell.data_ptr(), g.rad_j.data_ptr(), g.rad_s.data_ptr(), g.rad_n.data_ptr(),
                  g.cap_r, lib_p, layout.t_atom_row.data_ptr(), ws.dx.data_ptr(), ws.dx.shape[1],
-                 ws.forces4.data_ptr(), ws.status.data_ptr(), stream)
+                 ws.forces4.data_ptr(), g.aev_stage.data_ptr(), ws.status.data_ptr(), stream)
 
     def check_status(self, ws: Workspace, g: GraphBuffers) -> Optional[Tuple[int, int]]:
         """None if every list fitted, else the capacities to regrow to."""

@@ -216,6 +216,31 @@ int fennol_aev_backward(const float* xyzs, int natoms, const int* atom_sys,
                         int* status, void* stream);
 
 /*
+ * A forward/adjoint pair that shares the per-centre staging.  Both kernels
+ * first gather each centre's row, compute its edge vectors, distances and
+ * cutoffs, and sort the neighbours by species (ani.py:47-142 and the graph
+ * processors it reads); with these two calls the forward saves that staged
+ * neighbourhood to `stage` and the adjoint of the same step reads it back
+ * instead of recomputing it.  fennol_aev_forward_staged is fennol_aev_forward
+ * plus the save; fennol_aev_backward_staged is fennol_aev_backward (same
+ * result) reading `stage`, which must come from fennol_aev_forward_staged on
+ * the same positions, lists, capacity and parameters, with no other call
+ * writing it in between.  `stage` is device memory of
+ * fennol_aev_stage_bytes(natoms, capacity) bytes, 16-byte aligned.
+ */
+size_t fennol_aev_stage_bytes(int natoms, int capacity);
+int fennol_aev_forward_staged(const float* xyzs, int natoms, const int* atom_sys,
+                              const float* sys_cell, const int* nbr_j, const unsigned* nbr_shift,
+                              const int* nbr_count, int capacity, const fennol_aev_params* p,
+                              const int* atom_row, int out_kind, void* out, void* out_lo, int ld,
+                              void* stage, size_t stage_bytes, int* status, void* stream);
+int fennol_aev_backward_staged(const float* xyzs, int natoms, const int* atom_sys,
+                               const float* sys_cell, const int* nbr_j, const unsigned* nbr_shift,
+                               const int* nbr_count, int capacity, const fennol_aev_params* p,
+                               const int* atom_row, const float* daev, int ld, float* forces4,
+                               const void* stage, int* status, void* stream);
+
+/*
  * fennol_aev_backward that also writes, per centre atom i, the 3x3 sum over
  * its edges of r_ij (x) dE/dr_ij (atom_virial, float32 [natoms*9], row-major
  * a,b = r_a * g_b).  Summed per system (fennol_virial_reduce) this is the

@@ -104,3 +104,39 @@ def test_batched_equals_alone(pot32):
         e, f = pot32.energy_and_forces(s.coordinates, s.species, [s.natoms], c)
         assert abs(float(e[0]) - e_mix[b]) * HARTREE_TO_KCALMOL / s.natoms < 1e-6
         np.testing.assert_allclose(f.cpu().numpy(), f_mix[off[b]:off[b + 1]], atol=2e-5)
+
+
+def test_staged_adjoint_matches_unstaged(cuda_device):
+    """fennol_aev_backward_staged (reading the staging saved by
+    fennol_aev_forward_staged) gives the forces of fennol_aev_backward, and
+    the staged forward writes the same AEV rows as the plain one."""
+    from fennol_b200 import _lib
+    from fennol_b200._lib import call
+    from fennol_b200.potential import C_ptr, _ptr
+
+    pot = ANIPotential(precision="bf16x2", device=cuda_device, seed=0, bf16_weights=True)
+    s = water_box(6, seed=31)
+    x = torch.tensor(s.coordinates, dtype=torch.float32, device=cuda_device)
+    pot.energy_and_forces(x, s.species, [s.natoms], s.cell[None])
+    lay, g, ws = next(iter(pot._cache.values()))
+    st = torch.cuda.current_stream().cuda_stream
+    lp = C_ptr(pot.params)
+    args = (ws.xyzs.data_ptr(), lay.n, lay.t_atom_sys.data_ptr(), lay.t_cell.data_ptr(), g.rad_j.data_ptr(),
+            g.rad_s.data_ptr(), g.rad_n.data_ptr(), g.cap_r, lp, lay.t_atom_row.data_ptr())
+    rows = lay.t_atom_row.long()
+    call("fennol_aev_forward", *args, ws.aev_kind, ws.x.data_ptr(), _ptr(ws.x_lo), ws.x.shape[1],
+         ws.status.data_ptr(), st)
+    x_plain = ws.x[rows].clone()
+    call("fennol_aev_forward_staged", *args, ws.aev_kind, ws.x.data_ptr(), _ptr(ws.x_lo), ws.x.shape[1],
+         g.aev_stage.data_ptr(), g.aev_stage.numel(), ws.status.data_ptr(), st)
+    assert torch.equal(ws.x[rows], x_plain)
+    ws.dx.normal_()  # any dE/dAEV rows
+    f = []
+    for name, extra in (("fennol_aev_backward", ()), ("fennol_aev_backward_staged", (g.aev_stage.data_ptr(),))):
+        ws.forces4.zero_()
+        call(name, *args, ws.dx.data_ptr(), ws.dx.shape[1], ws.forces4.data_ptr(), *extra,
+             ws.status.data_ptr(), st)
+        f.append(ws.forces4[:lay.n, :3].cpu().numpy().copy())
+    assert int(ws.status[_lib.ST_ANG_OVERFLOW]) == 0
+    scale = np.abs(f[0]).max()
+    np.testing.assert_allclose(f[1], f[0], atol=1e-5 * scale, rtol=0)
