@@ -1002,10 +1002,7 @@ class _RowsView:
 
     def __init__(self, rows: NeighborRows):
         self.rad_j, self.rad_s, self.rad_n, self.cap_r = rows.j, rows.shift, rows.count, rows.capacity
-        # per-centre AEV staging shared by the forward and the adjoint of one call
-        n = max(int(rows.count.shape[0]), 1)
-        sb = _lib.load().fennol_aev_stage_bytes(n, int(rows.capacity))
-        self.aev_stage = torch.empty(int(sb), dtype=torch.uint8, device=rows.count.device)
+        self.aev_stage = None  # one-off rows: the plain forward/adjoint pair
 
 
 def _embedding_from_rows(ws: Workspace, layout: BatchLayout, width: int) -> torch.Tensor:

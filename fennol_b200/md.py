@@ -165,7 +165,7 @@ class MDEngine:
             grow = self.pot.check_status(self.ws, self.graph_buf)
             if grow is None:
                 break
-            self.graph_buf = GraphBuffers(self.layout, self.graph_buf.cutoff, self.skin, *grow)
+            self.graph_buf = self.graph_buf.regrown(self.layout, *grow)
         else:
             raise RuntimeError("neighbour capacity did not converge")
         self.x_ref.copy_(self.x)
@@ -268,7 +268,7 @@ class MDEngine:
         grow = self.pot.check_status(self.ws, self.graph_buf)
         if grow is None:
             return False
-        self.graph_buf = GraphBuffers(self.layout, self.graph_buf.cutoff, self.skin, *grow)
+        self.graph_buf = self.graph_buf.regrown(self.layout, *grow)
         self._graphs.clear()
         self.restore()
         self._initial_forces_from_current()

@@ -249,9 +249,14 @@ class BatchLayout:
 
 class GraphBuffers:
     """Neighbour rows of one layout: the build list (cutoff + skin) and, when
-    a skin is used, the radial list filtered from it."""
+    a skin is used, the radial list filtered from it.  With ``stage`` also the
+    per-centre AEV staging that the forward saves for the adjoint of the same
+    call (``fennol_aev_forward_staged``): worth its memory for buffers reused
+    over many calls (MD, a repeated single-point layout), not for one-off
+    batches."""
 
-    def __init__(self, layout: BatchLayout, cutoff: float, skin: float, cap: int, cap_radial: int):
+    def __init__(self, layout: BatchLayout, cutoff: float, skin: float, cap: int, cap_radial: int,
+                 stage: bool = False):
         dev = layout.device
         n = max(layout.n, 1)
         self.cutoff, self.skin = cutoff, skin
@@ -271,9 +276,14 @@ class GraphBuffers:
         else:
             self.cap_r = cap
             self.rad_j, self.rad_s, self.rad_n = self.nbr_j, self.nbr_s, self.nbr_n
-        # per-centre staging that the AEV forward saves for the adjoint of the same step
-        sb = _lib.load().fennol_aev_stage_bytes(n, self.cap_r)
-        self.aev_stage = torch.empty(int(sb), dtype=torch.uint8, device=dev)
+        self.aev_stage = None
+        if stage:
+            sb = _lib.load().fennol_aev_stage_bytes(n, self.cap_r)
+            self.aev_stage = torch.empty(int(sb), dtype=torch.uint8, device=dev)
+
+    def regrown(self, layout: BatchLayout, cap: int, cap_radial: int) -> "GraphBuffers":
+        """New buffers with larger row capacities and the same settings."""
+        return GraphBuffers(layout, self.cutoff, self.skin, cap, cap_radial, stage=self.aev_stage is not None)
 
     def build(self, layout: BatchLayout, coords: torch.Tensor, status: torch.Tensor, stream: int,
               enable_flag: Optional[torch.Tensor] = None):
@@ -411,7 +421,7 @@ class ANIPotential:
             cap = layout.estimate_capacity(rc + skin)
         if cap_radial is None:
             cap_radial = layout.estimate_capacity(rc) if skin > 0 else cap
-        g = GraphBuffers(layout, rc, skin, cap, cap_radial)
+        g = GraphBuffers(layout, rc, skin, cap, cap_radial, stage=True)
         ws = Workspace(self, layout)
         return g, ws
 
@@ -432,7 +442,8 @@ class ANIPotential:
         """AEV -> MLP -> energies (and adjoint -> forces) from the current radial list."""
         lib_p = C_ptr(self.params)
         n = layout.n
-        staged = want_forces and not want_virial  # the adjoint reuses the forward's staging
+        # the adjoint reuses the forward's staging when the buffers carry it
+        staged = want_forces and not want_virial and getattr(g, "aev_stage", None) is not None
         if staged:
             call("fennol_aev_forward_staged", ws.xyzs.data_ptr(), n, layout.t_atom_sys.data_ptr(),
                  layout.t_cell.data_ptr(), g.rad_j.data_ptr(), g.rad_s.data_ptr(), g.rad_n.data_ptr(),
@@ -460,12 +471,18 @@ class ANIPotential:
                  ws.forces4.data_ptr(), av.data_ptr(), ws.status.data_ptr(), stream)
             call("fennol_virial_reduce", av.data_ptr(), n, layout.t_sys_start.data_ptr(), layout.nsys,
                  float(self.unit_scale), vir.data_ptr(), stream)
-        elif want_forces:
+        elif staged:
             ws.forces4.zero_()
             call("fennol_aev_backward_staged", ws.xyzs.data_ptr(), n, layout.t_atom_sys.data_ptr(),
                  layout.t_cell.data_ptr(), g.rad_j.data_ptr(), g.rad_s.data_ptr(), g.rad_n.data_ptr(),
                  g.cap_r, lib_p, layout.t_atom_row.data_ptr(), ws.dx.data_ptr(), ws.dx.shape[1],
                  ws.forces4.data_ptr(), g.aev_stage.data_ptr(), ws.status.data_ptr(), stream)
+        elif want_forces:
+            ws.forces4.zero_()
+            call("fennol_aev_backward", ws.xyzs.data_ptr(), n, layout.t_atom_sys.data_ptr(),
+                 layout.t_cell.data_ptr(), g.rad_j.data_ptr(), g.rad_s.data_ptr(), g.rad_n.data_ptr(),
+                 g.cap_r, lib_p, layout.t_atom_row.data_ptr(), ws.dx.data_ptr(), ws.dx.shape[1],
+                 ws.forces4.data_ptr(), ws.status.data_ptr(), stream)
 
     def check_status(self, ws: Workspace, g: GraphBuffers) -> Optional[Tuple[int, int]]:
         """None if every list fitted, else the capacities to regrow to."""
@@ -541,14 +558,14 @@ class ANIPotential:
             if grow is None:
                 return ws
             self._graphs.pop(gkey, None)
-            g = GraphBuffers(layout, g.cutoff, g.skin, grow[0], grow[1])
+            g = g.regrown(layout, grow[0], grow[1])
             self._cache[key] = (layout, g, ws)
         for _attempt in range(4):
             self._launch_all(layout, g, ws, coords, stream, want_forces, want_virial)
             grow = self.check_status(ws, g)
             if grow is None:
                 break
-            g = GraphBuffers(layout, g.cutoff, g.skin, grow[0], grow[1])
+            g = g.regrown(layout, grow[0], grow[1])
             self._cache[key] = (layout, g, ws)
         else:
             raise RuntimeError("neighbour capacity did not converge")

@@ -457,9 +457,8 @@ class ServingEngine:
         self.force_scale = HARTREE_TO_KCALMOL / pot.unit_scale
         d0 = pot.mlp.dims[0]
         act = 2 * 2 if pot.precision != _lib.MLP_FP32 else 4
-        # AEV rows (hi+lo or fp32) + dE/dAEV + neighbour rows + per-atom state +
-        # the per-centre staging the AEV forward saves for the adjoint
-        self.bytes_per_atom = d0 * (act + 4) + 8 * 128 + 256 + (20 * 128 + 28 * 96 + 128)
+        # AEV rows (hi+lo or fp32) + dE/dAEV + neighbour rows + per-atom state
+        self.bytes_per_atom = d0 * (act + 4) + 8 * 128 + 256
         self.bytes_per_atom_md = self.bytes_per_atom + 8 * 96 + 128
         self.bytes_in_flight = 0
         self.results: List[ServeResult] = []
