@@ -245,7 +245,13 @@ def kernel_times(pot, eng, reps=20):
     ws.forces4.zero_()
     eng._initial_forces_from_current()
     mean_nbr = float(g.rad_n[:lay.n].float().mean())
-    return out, mean_nbr
+    # angular neighbours (within the angular cutoff) of the current positions, periodic cube
+    from scipy.spatial import cKDTree
+    box_len = float(np.asarray(eng.cell).reshape(-1, 3, 3)[0, 0, 0])
+    xyz = np.mod(eng.x.cpu().numpy(), box_len)
+    tree = cKDTree(xyz, boxsize=box_len)
+    mean_ang = float(np.mean(tree.query_ball_point(xyz, r=pot.aev_cfg.angular_cutoff, return_length=True)) - 1.0)
+    return out, mean_nbr, mean_ang
 
 
 def profile_traffic(kernel: str, workload: str):
@@ -583,15 +589,19 @@ def main():
     extras = world == 1
     if rank == 0:
         hbm, tf_burst, tf_sust, src = measured_peaks()
-        kt, mean_nbr = kernel_times(pot, eng)
+        kt, mean_nbr, mean_ang = kernel_times(pot, eng)
         mlp_ms = kt["mlp"]
         flops = MLP_FLOP_PER_ATOM * box.natoms * w["n_models"]
         mlp_tf = flops / (mlp_ms * 1e-3) / 1e12
+        # the per-centre staging record the forward writes and the adjoint reads:
+        # 20 B per radial edge, 28 B per angular neighbour, 4 S counters (S = 7)
+        rec = 20 * mean_nbr + 28 * mean_ang + 4 * 4 * 7
         # algorithmic bytes per atom of the adjoint: its dE/dAEV row (float32),
-        # its neighbour row (index + packed shift), its position in and force out
-        bwd_bytes = box.natoms * (1008 * 4 + mean_nbr * 8 + 16 + 16)
-        # forward: neighbour row and position in, AEV row out (BF16 hi + lo or float32)
-        fwd_bytes = box.natoms * (mean_nbr * 8 + 16 + 1008 * (2 if precision == "bf16" else 4))
+        # its staging record, the neighbour indices of its row and its force out
+        bwd_bytes = box.natoms * (1008 * 4 + rec + mean_nbr * 4 + 16)
+        # forward: neighbour row and position in, AEV row out (BF16 hi + lo or
+        # float32), staging record out
+        fwd_bytes = box.natoms * (mean_nbr * 8 + 16 + 1008 * (2 if precision == "bf16" else 4) + rec)
         kernels = {
             "aev_backward": {"ms_per_launch": kt["aev_backward"], "bound": "hbm",
                              "algorithmic_bytes_per_launch": bwd_bytes,
@@ -608,6 +618,7 @@ def main():
             k["frac"] = k["achieved"] / k["peak"]
         res["kernels"] = kernels
         res["kernels"]["mean_radial_neighbors"] = mean_nbr
+        res["kernels"]["mean_angular_neighbors"] = mean_ang
         top = max(("aev_backward", "aev_forward", "mlp"), key=lambda k: kernels[k]["ms_per_launch"])
         kd = kernels[top]
         names = {"aev_backward": "k_aev_backward", "aev_forward": "k_aev_forward", "mlp": "k_mlp_fused"}
