@@ -172,6 +172,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
   __syncthreads();
   fence_after_sync();
   const uint32_t tmem = bars->tmem_slot;
+  // Launched as a programmatic dependent of the AEV forward: the set-up above
+  // (barriers, TMEM) touches no global memory and overlaps that kernel's last
+  // wave; every role reads or writes global memory only after this wait.
+  pdl_wait();
 
   const uint32_t x_tx = kAtom * (1 + p.a_lo) + (uint32_t)p.d1 * BK * 2;
 
@@ -651,7 +655,7 @@ int fnl_mlp_fused(int precision, int rows, int ntiles, const int* tile_species, 
   }
   if (ntiles <= 0) return FENNOL_OK;
   const int grid = ntiles < sm_count() ? ntiles : sm_count();
-  k_mlp_fused<<<grid, kThreads, smem, st>>>(maps, p);
+  FNL_LAUNCH_PDL(k_mlp_fused, dim3(grid), dim3(kThreads), smem, st, maps, p);
   FNL_CHECK_LAUNCH();
   return FENNOL_OK;
 }
