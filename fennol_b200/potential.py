@@ -438,8 +438,11 @@ class ANIPotential:
 
     # --------------------------------------------------------------- launches
     def launch_forces(self, layout: BatchLayout, g: GraphBuffers, ws: Workspace, stream: int,
-                      want_forces: bool = True, want_virial: bool = False):
-        """AEV -> MLP -> energies (and adjoint -> forces) from the current radial list."""
+                      want_forces: bool = True, want_virial: bool = False,
+                      ghost_rows: Optional[torch.Tensor] = None):
+        """AEV -> MLP -> energies (and adjoint -> forces) from the current radial
+        list.  ``ghost_rows``: MLP rows of centres whose energy does not count
+        (their row energy and dE/dAEV are cleared before the sum and the adjoint)."""
         lib_p = C_ptr(self.params)
         n = layout.n
         # the adjoint reuses the forward's staging when the buffers carry it
@@ -459,6 +462,9 @@ class ANIPotential:
              layout.t_tile_species.data_ptr(), layout.t_tile_row.data_ptr(), C_ptr(self.mlp.struct),
              ws.x.data_ptr(), _ptr(ws.x_lo), ws.e_rows.data_ptr(), ws.dx.data_ptr(),
              ws.mlp_ws.data_ptr(), ws.mlp_ws.numel(), stream)
+        if ghost_rows is not None and ghost_rows.numel() > 0:
+            ws.e_rows.index_fill_(0, ghost_rows, 0.0)
+            ws.dx.index_fill_(0, ghost_rows, 0.0)
         call("fennol_energy_reduce", ws.e_rows.data_ptr(), layout.t_atom_row.data_ptr(), n,
              layout.t_sys_start.data_ptr(), layout.nsys, float(self.unit_scale), ws.energy.data_ptr(),
              ws.e_atom.data_ptr(), ws.energy_ws.data_ptr(), ws.energy_ws.numel(), stream)
@@ -514,11 +520,16 @@ class ANIPotential:
         return self._cache[key]
 
     def energy_and_forces(self, coordinates, species, natoms=None, cells=None,
-                          want_forces: bool = True):
+                          want_forces: bool = True, centres: Optional[int] = None):
         """Energies [B] (float64) and forces [N,3] (float32) as torch tensors
         on the device.  ``coordinates`` may be a host array or a device
-        tensor ([N,3], Angstrom); ``species`` are atomic numbers."""
-        ws = self._evaluate(coordinates, species, natoms, cells, want_forces, False)
+        tensor ([N,3], Angstrom); ``species`` are atomic numbers.
+
+        ``centres`` (one system only): only the first ``centres`` atoms are
+        centres whose atomic energies count; the others are ghost atoms that
+        only shape those centres' environments (spatial decomposition).  The
+        forces are then -d/dx of the owned centres' energy, on all atoms."""
+        ws = self._evaluate(coordinates, species, natoms, cells, want_forces, False, centres)
         n = self._cache[next(iter(self._cache))][0].n
         return ws.energy, (ws.forces[:n] if want_forces else None)
 
@@ -530,11 +541,16 @@ class ANIPotential:
         n = self._cache[next(iter(self._cache))][0].n
         return ws.energy, ws.forces[:n], ws.virial
 
-    def _evaluate(self, coordinates, species, natoms, cells, want_forces: bool, want_virial: bool):
+    def _evaluate(self, coordinates, species, natoms, cells, want_forces: bool, want_virial: bool,
+                  centres: Optional[int] = None):
         species = np.asarray(species)
         if natoms is None:
             natoms = [species.shape[0]]
         natoms = tuple(int(v) for v in np.asarray(natoms).reshape(-1))
+        if centres is not None:
+            if len(natoms) != 1 or not 0 <= int(centres) <= natoms[0]:
+                raise ValueError("centres applies to a single system and must lie in [0, natoms]")
+            centres = None if int(centres) == natoms[0] else int(centres)
         if cells is None:
             cell_key = None
         elif isinstance(cells, (list, tuple)):
@@ -548,7 +564,7 @@ class ANIPotential:
             coords = coords.to(self.device, non_blocking=True)
         coords = coords.contiguous()
         stream = _stream(self.device)
-        gkey = (key, bool(want_forces), bool(want_virial))
+        gkey = (key, bool(want_forces), bool(want_virial), centres)
         rec = self._graphs.get(gkey) if self.use_graphs else None
         if rec is not None and rec["g"] is g:
             # same batch as the last calls: one graph launch for the whole evaluation
@@ -561,7 +577,7 @@ class ANIPotential:
             g = g.regrown(layout, grow[0], grow[1])
             self._cache[key] = (layout, g, ws)
         for _attempt in range(4):
-            self._launch_all(layout, g, ws, coords, stream, want_forces, want_virial)
+            self._launch_all(layout, g, ws, coords, stream, want_forces, want_virial, centres)
             grow = self.check_status(ws, g)
             if grow is None:
                 break
@@ -573,11 +589,11 @@ class ANIPotential:
             calls = self._calls.get(gkey, 0) + 1
             self._calls = {gkey: calls}
             if calls >= 2:  # a repeated batch: capture it once
-                self._capture(gkey, layout, g, ws, coords, want_forces, want_virial)
+                self._capture(gkey, layout, g, ws, coords, want_forces, want_virial, centres)
         return ws
 
     def _launch_all(self, layout: BatchLayout, g: GraphBuffers, ws: Workspace, coords: torch.Tensor,
-                    stream: int, want_forces: bool, want_virial: bool = False):
+                    stream: int, want_forces: bool, want_virial: bool = False, centres: Optional[int] = None):
         """Every launch of one evaluation: pack, list build and filter, AEV,
         MLP, energy sum, adjoint and force finalisation."""
         ws.status.zero_()
@@ -585,17 +601,18 @@ class ANIPotential:
              ws.xyzs.data_ptr(), stream)
         g.build(layout, coords, ws.status, stream)
         g.filter(layout, coords, ws.status, stream)
-        self.launch_forces(layout, g, ws, stream, want_forces, want_virial)
+        ghost_rows = None if centres is None else layout.t_atom_row[centres:layout.n].long()
+        self.launch_forces(layout, g, ws, stream, want_forces, want_virial, ghost_rows)
         if want_forces:
             call("fennol_forces_finalize", ws.forces4.data_ptr(), layout.n, float(self.unit_scale),
                  ws.forces.data_ptr(), stream)
 
-    def _capture(self, gkey, layout, g, ws, coords, want_forces, want_virial):
+    def _capture(self, gkey, layout, g, ws, coords, want_forces, want_virial, centres=None):
         buf = torch.empty_like(coords)
         buf.copy_(coords)
         graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(graph):
-            self._launch_all(layout, g, ws, buf, _stream(self.device), want_forces, want_virial)
+            self._launch_all(layout, g, ws, buf, _stream(self.device), want_forces, want_virial, centres)
         self._graphs = {gkey: {"graph": graph, "coords": buf, "g": g}}
         # the replay recomputes the same values; results of this call stay valid
 
