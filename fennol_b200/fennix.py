@@ -975,6 +975,14 @@ class FENNIX:
         fac = self._unit_factor(unit)
         return out["total_energy"] * fac, out["forces"] * fac, out["virial_tensor"] * fac, out
 
+    def set_energy_terms(self, energy_terms, jit: bool = True) -> None:
+        """Select the energy terms of ``total_energy`` (``fennix.py:180-270``):
+        a name or a list of names; None or an empty list gives zero energies
+        and forces.  ``jit`` is accepted for signature compatibility."""
+        if isinstance(energy_terms, str):
+            energy_terms = [energy_terms]
+        self.energy_terms = list(energy_terms) if energy_terms else None
+
     def get_model(self):
         return (self.aev_module, self.net_module), self.variables
 
