@@ -435,33 +435,51 @@ k_filter(const float* __restrict__ coords, int n, const int* __restrict__ atom_s
   if (cnt > in_cap) cnt = in_cap;
   size_t ib = (size_t)i * in_cap, ob = (size_t)i * out_cap;
   int count = 0;
-  for (int k0 = 0; k0 < cnt; k0 += 32) {
-    int k = k0 + lane;
-    bool keep = false;
-    int j = 0;
-    unsigned sh = 0;
-    if (k < cnt) {
-      j = in_j[ib + k];
-      sh = in_shift[ib + k];
-      float vx = __fsub_rn(coords[3 * j], xi);
-      float vy = __fsub_rn(coords[3 * j + 1], yi);
-      float vz = __fsub_rn(coords[3 * j + 2], zi);
-      if (sh && c) {
-        int sx, sy, sz;
-        unpack_shift(sh, sx, sy, sz);
-        add_shift(vx, vy, vz, (float)sx, (float)sy, (float)sz, c);
-      }
-      keep = dist2_exact(vx, vy, vz) < rc2;
+  // up to kFilterRounds 32-entry rounds at a time: all their index and
+  // position loads are in flight together, then the tests and the ordered
+  // ballot compaction run round by round (same rows as one round at a time)
+  constexpr int kFilterRounds = 4;
+  for (int k0 = 0; k0 < cnt; k0 += 32 * kFilterRounds) {
+    int j[kFilterRounds];
+    unsigned sh[kFilterRounds];
+#pragma unroll
+    for (int u = 0; u < kFilterRounds; ++u) {
+      const int k = k0 + 32 * u + lane;
+      j[u] = k < cnt ? in_j[ib + k] : -1;
+      sh[u] = k < cnt ? in_shift[ib + k] : 0u;
     }
-    unsigned m = __ballot_sync(0xffffffffu, keep);
-    if (keep) {
-      int pos = count + warp_exclusive_prefix(m, lane);
-      if (pos < out_cap) {
-        out_j[ob + pos] = j;
-        out_shift[ob + pos] = sh;
-      }
+    float px[kFilterRounds], py[kFilterRounds], pz[kFilterRounds];
+#pragma unroll
+    for (int u = 0; u < kFilterRounds; ++u) {
+      const int jj = j[u] < 0 ? i : j[u];
+      px[u] = coords[3 * jj];
+      py[u] = coords[3 * jj + 1];
+      pz[u] = coords[3 * jj + 2];
     }
-    count += __popc(m);
+#pragma unroll
+    for (int u = 0; u < kFilterRounds; ++u) {
+      bool keep = false;
+      if (j[u] >= 0) {
+        float vx = __fsub_rn(px[u], xi);
+        float vy = __fsub_rn(py[u], yi);
+        float vz = __fsub_rn(pz[u], zi);
+        if (sh[u] && c) {
+          int sx, sy, sz;
+          unpack_shift(sh[u], sx, sy, sz);
+          add_shift(vx, vy, vz, (float)sx, (float)sy, (float)sz, c);
+        }
+        keep = dist2_exact(vx, vy, vz) < rc2;
+      }
+      unsigned m = __ballot_sync(0xffffffffu, keep);
+      if (keep) {
+        int pos = count + warp_exclusive_prefix(m, lane);
+        if (pos < out_cap) {
+          out_j[ob + pos] = j[u];
+          out_shift[ob + pos] = sh[u];
+        }
+      }
+      count += __popc(m);
+    }
   }
   if (lane == 0) {
     out_count[i] = count < out_cap ? count : out_cap;
