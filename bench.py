@@ -43,8 +43,9 @@ MLP_FLOP_PER_ATOM = 2 * (1008 * 256 + 256 * 192 + 192 * 160 + 160 * 1) * 2  # fw
 WORKLOADS = {
     "water12k": dict(n_side=16, n_models=1, thermostat="LGV", desc=(
         "water box 12,288 atoms (4096 H2O, 49.7 A cube), Langevin 300 K gamma 1/ps, dt 0.5 fs, "
-        "skin 1.0 A, list rebuilt every nblist_stride steps (FeNNol's rule, 40 steps) with every "
-        "step checked on the device (displacement > skin/2 rolls back and shortens the stride), "
+        "skin 1.0 A, list rebuilt every nblist_stride steps (FeNNol's rule gives 40 at 0.5 fs) with "
+        "every step checked on the device (an atom moved > skin/2 since the rebuild: roll back and "
+        "shorten the stride; the value used is in neighbour_list), "
         "ANI-2x 7-species random-init model "
         "(MD: last layer x0.02)")),
     "water98k": dict(n_side=32, n_models=8, thermostat="NVE", desc=(
