@@ -118,3 +118,29 @@ def test_single_rank_is_the_plain_box():
 def test_narrow_slabs_are_rejected():
     with pytest.raises(ValueError):
         SlabPlan(np.diag([18.0, 18.0, 18.0]), 4, 5.2)
+
+
+def test_plan_wraps_coordinates_and_faces():
+    cell = np.diag([30.0, 20.0, 20.0])
+    plan = SlabPlan(cell, 3, 5.2)  # slabs of 10 A
+    x = np.array([[-1.0, 0.0, 0.0],    # wraps to 29: rank 2
+                  [10.0, 0.0, 0.0],    # on the 0|1 face: rank 1
+                  [29.999, 5.0, -3.0],  # rank 2
+                  [31.0, 25.0, 0.0],   # wraps to 1: rank 0
+                  [0.0, 0.0, 0.0]])
+    np.testing.assert_array_equal(plan.owners(x), [2, 1, 2, 0, 0])
+    loc = plan.local(x, 0)
+    owned = set(loc.ids[:loc.n_owned].tolist())
+    assert owned == {3, 4}
+    # rank 0's local x: owned atoms in [halo, halo + width), everything inside the local cell
+    assert np.all(loc.coordinates[:loc.n_owned, 0] >= 5.2) and np.all(loc.coordinates[:loc.n_owned, 0] < 15.2)
+    assert np.all(loc.coordinates[:, 0] >= 0.0) and np.all(loc.coordinates[:, 0] < loc.cell[0, 0])
+    assert np.all(loc.coordinates[:, 1:] >= 0.0) and np.all(loc.coordinates[:, 1:] < 20.0)
+    # atoms 0 and 2 (x = 29, 29.999) sit within the halo below rank 0's lower face
+    assert {0, 2} <= set(loc.ids[loc.n_owned:].tolist())
+
+
+def test_plan_rejects_triclinic_cells():
+    cell = np.array([[20.0, 0.0, 0.0], [3.0, 20.0, 0.0], [0.0, 0.0, 20.0]])
+    with pytest.raises(ValueError):
+        SlabPlan(cell, 2, 5.2)
