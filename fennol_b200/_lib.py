@@ -31,9 +31,11 @@ ST_ANG_OVERFLOW, ST_ANG_MAXCOUNT, ST_CELL_OVERFLOW, ST_REBUILD_COUNT = 4, 5, 6, 
 PBC_NONE, PBC_MINIMUM_IMAGE, PBC_GENERAL = 0, 1, 2
 MAX_ANGULAR_NEIGHBORS = 96
 
-AEV_F32, AEV_BF16, AEV_BF16X2 = 0, 1, 2
-MLP_FP32, MLP_BF16, MLP_BF16X2, MLP_BF16X3 = 0, 1, 2, 3
-PRECISIONS = {"fp32": MLP_FP32, "bf16": MLP_BF16, "bf16x2": MLP_BF16X2, "bf16x3": MLP_BF16X3}
+AEV_F32, AEV_BF16, AEV_BF16X2, AEV_F16X2 = 0, 1, 2, 3
+MLP_FP32, MLP_BF16, MLP_BF16X2, MLP_BF16X3, MLP_F16X3X1, MLP_F16X3X2 = 0, 1, 2, 3, 4, 5
+PRECISIONS = {"fp32": MLP_FP32, "bf16": MLP_BF16, "bf16x2": MLP_BF16X2, "bf16x3": MLP_BF16X3,
+              "f16x3x1": MLP_F16X3X1, "f16x3x2": MLP_F16X3X2}
+F16_FORMS = (MLP_F16X3X1, MLP_F16X3X2)
 
 _ERRNAMES = {ERR_INVALID: "invalid argument", ERR_CUDA: "CUDA launch failure",
              ERR_UNSUPPORTED: "unsupported parameters", ERR_WORKSPACE: "workspace too small",
@@ -63,7 +65,8 @@ class MLPWeights(C.Structure):
                 ("celu_alpha", C.c_float),
                 ("w32", C.c_void_p * 4), ("b32", C.c_void_p * 4),
                 ("wt_hi", C.c_void_p * 4), ("wt_lo", C.c_void_p * 4),
-                ("w_hi", C.c_void_p * 4), ("w_lo", C.c_void_p * 4)]
+                ("w_hi", C.c_void_p * 4), ("w_lo", C.c_void_p * 4),
+                ("f16_scale", C.c_void_p)]
 
 
 P = C.c_void_p

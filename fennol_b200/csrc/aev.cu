@@ -400,6 +400,10 @@ __device__ __forceinline__ float transpose_reduce32(float* v, int lane) {
 __device__ __forceinline__ void store_feature(int out_kind, void* out, void* out_lo, size_t idx, float v) {
   if (out_kind == FENNOL_AEV_F32) {
     ((float*)out)[idx] = v;
+  } else if (out_kind == FENNOL_AEV_F16X2) {
+    const __half hi = __float2half_rn(v);
+    ((__half*)out)[idx] = hi;
+    ((__half*)out_lo)[idx] = __float2half_rn(v - __half2float(hi));
   } else {
     __nv_bfloat16 hi = to_bf16(v);
     ((__nv_bfloat16*)out)[idx] = hi;
@@ -1042,9 +1046,10 @@ static int aev_forward_launch(const float* xyzs, int natoms, const int* atom_sys
   if (natoms == 0) return FENNOL_OK;
   if (!xyzs || !atom_sys || !nbr_j || !nbr_shift || !nbr_count || !atom_row || !out)
     return FENNOL_ERR_INVALID;
-  if (out_kind != FENNOL_AEV_F32 && out_kind != FENNOL_AEV_BF16 && out_kind != FENNOL_AEV_BF16X2)
+  if (out_kind != FENNOL_AEV_F32 && out_kind != FENNOL_AEV_BF16 && out_kind != FENNOL_AEV_BF16X2 &&
+      out_kind != FENNOL_AEV_F16X2)
     return FENNOL_ERR_INVALID;
-  if (out_kind == FENNOL_AEV_BF16X2 && !out_lo) return FENNOL_ERR_INVALID;
+  if ((out_kind == FENNOL_AEV_BF16X2 || out_kind == FENNOL_AEV_F16X2) && !out_lo) return FENNOL_ERR_INVALID;
   if ((size_t)kAevWarps * stage_bytes(capacity) > 200 * 1024) return FENNOL_ERR_UNSUPPORTED;
   int blocks = (natoms + kAevWarps - 1) / kAevWarps;
   bool launched = dispatch(K, [&](auto ks) {

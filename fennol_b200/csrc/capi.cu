@@ -14,8 +14,11 @@ static bool weights_ok(int precision, const fennol_mlp_weights* w) {
     for (int l = 0; l < 3; ++l) {
       if (!w->wt_hi[l] || !w->w_hi[l]) return false;
       if (precision == FENNOL_MLP_BF16X3 && (!w->wt_lo[l] || !w->w_lo[l])) return false;
+      if ((precision == FENNOL_MLP_F16X3X1 || precision == FENNOL_MLP_F16X3X2) && !w->wt_lo[l]) return false;
+      if (precision == FENNOL_MLP_F16X3X2 && !w->w_lo[l]) return false;
     }
   }
+  if ((precision == FENNOL_MLP_F16X3X1 || precision == FENNOL_MLP_F16X3X2) && !w->f16_scale) return false;
   return true;
 }
 
@@ -30,7 +33,7 @@ extern "C" int fennol_mlp_energy_grad(int precision, int rows, int ntiles, const
                                       const int* tile_row, const fennol_mlp_weights* w, const void* x,
                                       const void* x_lo, float* e_rows, float* dx, void* workspace,
                                       size_t workspace_bytes, void* stream) {
-  if (precision < FENNOL_MLP_FP32 || precision > FENNOL_MLP_BF16X3) return FENNOL_ERR_INVALID;
+  if (precision < FENNOL_MLP_FP32 || precision > FENNOL_MLP_F16X3X2) return FENNOL_ERR_INVALID;
   if (!weights_ok(precision, w)) return FENNOL_ERR_INVALID;
   if (rows < 0 || ntiles < 0 || rows % 128 != 0 || ntiles * 128 > rows) return FENNOL_ERR_INVALID;
   if (ntiles == 0) return FENNOL_OK;

@@ -3,6 +3,7 @@
 #include <utility>
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <stdint.h>
 
 #include "fennol_b200.h"

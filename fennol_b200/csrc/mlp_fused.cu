@@ -7,15 +7,24 @@
 //     L1 X.W1  L2 H1.W2  L3 H2.W3 (+ energy head)  B3 G3.W3^T  B2 G2.W2^T  B1 G1.W1^T
 // keeping the activations on chip:
 //   * warp 0 (one thread) streams the AEV tile and W1^T through a 3-stage TMA
-//     ring that aliases the activation buffer and the weight ring, then all
-//     other weights through the 2-stage weight ring;
+//     ring (2 stages when the W1^T low parts come along) that aliases the
+//     activation buffer and the weight ring, then all other weights through
+//     the 2-stage weight ring;
 //   * warp 1 owns the 512 TMEM columns (two 256-column FP32 accumulators used
 //     alternately) and one thread issues tcgen05.mma / tcgen05.commit;
 //   * warps 2-9 are the epilogue: they read an accumulator (tcgen05.ld, one
 //     row per thread, two warps per lane quarter), apply bias + CELU, the energy
-//     head, or CELU' masks, and write the next A operand as BF16 hi + lo pairs
-//     straight into shared memory in the 128-byte-swizzled K-major layout the
-//     MMA descriptors expect (fence.proxy.async before the MMA reads it).
+//     head, or CELU' masks, and write the next A operand as 16-bit hi (+ lo)
+//     pairs straight into shared memory in the 128-byte-swizzled K-major
+//     layout the MMA descriptors expect (fence.proxy.async before the MMA
+//     reads it).
+// Operand forms: BF16 (A hi, optionally A lo; weights BF16) and FP16 (the
+// kernel template's F16 flag).  The FP16 forms split the activations and the
+// power-of-two-scaled float32 weights into float16 hi + lo: the forward GEMMs
+// run A_hi W_hi + A_lo W_hi + A_hi W_lo, the input-gradient GEMMs G_hi W_hi
+// (+ G_hi W_lo).  Each epilogue divides its accumulator by the layer's weight
+// scale; the backward chain carries the power-of-two scale of the last layer's
+// kernel until dX.
 // CELU' of layers 1-2 (needed by the backward) goes to a per-CTA scratch in
 // global memory that stays L2 resident.  The ensemble is processed model by
 // model inside the CTA, so the per-row energy and dE/dAEV sums are
@@ -42,8 +51,12 @@ constexpr int kWStages = 2;
 constexpr uint32_t kWStage = 256 * BK * 2;        // 32 KB
 constexpr uint32_t kXStage = kActBytes / 2;       // 64 KB: A hi | A lo | B (<= 256 rows)
 // L1 ring: stages 0-1 alias the activation buffer, stage 2 the weight ring
-// (idle while L1 streams); stage s starts at act + s * kXStage
+// (idle while L1 streams); stage s starts at act + s * kXStage.  With the W1^T
+// low parts a stage is A hi | A lo | B hi | B lo (96 KB) and the ring has two
+// stages, the second one aliasing the weight ring.
 constexpr int kXStages = 3;
+constexpr uint32_t kXStageWide = 6 * kAtom;       // 96 KB
+constexpr int kXStagesWide = 2;
 constexpr uint32_t kXpose = 8 * 32 * 32 * 4;      // per-epilogue-warp 32x32 dX staging tiles: 32 KB
 constexpr uint32_t kSmemMain = kActBytes + kWStages * kWStage + kXpose;  // 224 KB
 constexpr uint64_t kTimeoutNs = 2000000000ull;
@@ -53,8 +66,14 @@ struct FusedParams {
   const int* tile_species;
   const int* tile_row;
   int d0, d1, d2, d3;
-  int a_lo;
+  int a_lo;   // forward A operands (X, H1, H2) carry a lo part
+  int g_lo;   // input-gradient A operands (G3, G2, G1) carry a lo part
+  int wf_lo;  // forward GEMMs add A_hi x W_lo
+  int wb_lo;  // input-gradient GEMMs add G_hi x W_lo
+  int xstages;
+  uint32_t xstage;
   float alpha, inv_models;
+  const float4* scales;  // F16 forms: per group (s_W1, s_W2, s_W3, s_w4) powers of two
   const float* b1;
   const float* b2;
   const float* b3;
@@ -68,6 +87,7 @@ struct FusedParams {
 
 struct Maps {
   CUtensorMap x, xlo, w1t, w2t, w3t, w3, w2, w1;
+  CUtensorMap w1t_lo, w2t_lo, w3t_lo, w3_lo, w2_lo, w1_lo;  // low parts (unused maps alias the high ones)
   CUtensorMap dx;  // FP32 [rows][d0], 32 x 32 boxes, 128-byte swizzle
 };
 
@@ -108,19 +128,28 @@ __device__ __forceinline__ bool wait_bar(uint64_t* bar, uint32_t parity, volatil
   }
 }
 
-// Write 32 consecutive columns [n, n+32) of row r as BF16 hi (+ lo) into the
-// swizzled K-major activation buffer.
+// Write 32 consecutive columns [n, n+32) of row r as 16-bit hi (+ lo) into the
+// swizzled K-major activation buffer (BF16, or FP16 when F16).
+template <bool F16>
 __device__ __forceinline__ void act_store(uint8_t* act, int r, int n, const float* v, bool with_lo) {
   uint32_t h[16], l[16];
 #pragma unroll
   for (int k = 0; k < 16; ++k) {
     // one paired conversion per two columns for the high parts and one for the
     // residuals (round to nearest each, as two single conversions would)
-    const __nv_bfloat162 hb = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]);
-    const float2 hf = __bfloat1622float2(hb);
-    const __nv_bfloat162 lb = __floats2bfloat162_rn(v[2 * k] - hf.x, v[2 * k + 1] - hf.y);
-    h[k] = *reinterpret_cast<const uint32_t*>(&hb);
-    l[k] = *reinterpret_cast<const uint32_t*>(&lb);
+    if constexpr (F16) {
+      const __half2 hb = __floats2half2_rn(v[2 * k], v[2 * k + 1]);
+      const float2 hf = __half22float2(hb);
+      const __half2 lb = __floats2half2_rn(v[2 * k] - hf.x, v[2 * k + 1] - hf.y);
+      h[k] = *reinterpret_cast<const uint32_t*>(&hb);
+      l[k] = *reinterpret_cast<const uint32_t*>(&lb);
+    } else {
+      const __nv_bfloat162 hb = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]);
+      const float2 hf = __bfloat1622float2(hb);
+      const __nv_bfloat162 lb = __floats2bfloat162_rn(v[2 * k] - hf.x, v[2 * k + 1] - hf.y);
+      h[k] = *reinterpret_cast<const uint32_t*>(&hb);
+      l[k] = *reinterpret_cast<const uint32_t*>(&lb);
+    }
   }
   const int atom = n >> 6;
   const int j0 = (n & 63) >> 3;
@@ -135,6 +164,7 @@ __device__ __forceinline__ void act_store(uint8_t* act, int r, int n, const floa
   }
 }
 
+template <bool F16>
 __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant__ Maps maps, const FusedParams p) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -145,6 +175,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
   volatile int* abort_flag = &bars->abort_flag;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int M = p.n_models;
+  const int XS = p.xstages;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kXStages; ++s) {
@@ -177,7 +208,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
   // wave; every role reads or writes global memory only after this wait.
   pdl_wait();
 
-  const uint32_t x_tx = kAtom * (1 + p.a_lo) + (uint32_t)p.d1 * BK * 2;
+  const uint32_t x_tx = kAtom * (1 + p.a_lo) + (uint32_t)p.d1 * BK * 2 * (1 + p.wf_lo);
 
   if (warp == 0) {
     // ------------------------------------------------------------------ TMA producer
@@ -192,36 +223,44 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
           const int g = m * p.n_species + sp;
           if (item > 0 && !(ok = wait_bar(&bars->act_free, (item - 1) & 1, abort_flag, p.err))) break;
           for (int kc = 0; kc < p.d0 / BK; ++kc, ++xq) {
-            const int s = xq % kXStages;
-            const uint32_t u = xq / kXStages;
+            const int s = xq % XS;
+            const uint32_t u = xq / XS;
             if (u > 0 && !(ok = wait_bar(&bars->x_empty[s], (u - 1) & 1, abort_flag, p.err))) break;
-            uint8_t* st = act + s * kXStage;
+            uint8_t* st = act + s * p.xstage;
             mbar_expect_tx(&bars->x_full[s], x_tx);
             tma_load_2d(&maps.x, &bars->x_full[s], st, kc * BK, row0);
             if (p.a_lo) tma_load_2d(&maps.xlo, &bars->x_full[s], st + kAtom, kc * BK, row0);
             tma_load_2d(&maps.w1t, &bars->x_full[s], st + 2 * kAtom, kc * BK, g * p.d1);
+            if (p.wf_lo) tma_load_2d(&maps.w1t_lo, &bars->x_full[s], st + 4 * kAtom, kc * BK, g * p.d1);
           }
           if (!ok) break;
-          // the weight ring is L1 stage 2: its last chunk of this item must have
-          // been consumed (d0 / BK >= 3, so the item used stage 2)
+          // the weight ring lies in the last L1 stage: its last chunk of this
+          // item must have been consumed (d0 / BK >= 3, so the item used it)
           {
-            const uint32_t last = xq - 1 - ((xq - 1 - 2) % kXStages);
-            if (!(ok = wait_bar(&bars->x_empty[2], (last / kXStages) & 1, abort_flag, p.err))) break;
+            const int rs = XS - 1;
+            const uint32_t last = xq - 1 - ((xq - 1 - rs) % XS);
+            if (!(ok = wait_bar(&bars->x_empty[rs], (last / XS) & 1, abort_flag, p.err))) break;
           }
           // weight chunks of the remaining GEMMs, in MMA order
+          // (a GEMM with weight low parts takes the hi and lo chunks of each K step)
           const CUtensorMap* wm[5] = {&maps.w2t, &maps.w3t, &maps.w3, &maps.w2, &maps.w1};
+          const CUtensorMap* wml[5] = {&maps.w2t_lo, &maps.w3t_lo, &maps.w3_lo, &maps.w2_lo, &maps.w1_lo};
           const int rows_g[5] = {p.d2, p.d3, p.d2, p.d1, p.d0};
           const int box[5] = {p.d2, p.d3, p.d2, p.d1, 256};
           const int nk[5] = {p.d1 / BK, p.d2 / BK, p.d3 / BK, p.d2 / BK, p.d1 / BK};
           const int nchunk[5] = {1, 1, 1, 1, p.d0 / 256};
+          const int nt[5] = {1 + p.wf_lo, 1 + p.wf_lo, 1 + p.wb_lo, 1 + p.wb_lo, 1 + p.wb_lo};
           for (int jb = 0; jb < 5 && ok; ++jb) {
             for (int c = 0; c < nchunk[jb] && ok; ++c) {
-              for (int kc = 0; kc < nk[jb]; ++kc, ++wq) {
-                const int s = wq % kWStages;
-                const uint32_t u = wq / kWStages;
-                if (u > 0 && !(ok = wait_bar(&bars->w_empty[s], (u - 1) & 1, abort_flag, p.err))) break;
-                mbar_expect_tx(&bars->w_full[s], (uint32_t)box[jb] * BK * 2);
-                tma_load_2d(wm[jb], &bars->w_full[s], wring + s * kWStage, kc * BK, g * rows_g[jb] + c * 256);
+              for (int kc = 0; kc < nk[jb] && ok; ++kc) {
+                for (int t = 0; t < nt[jb]; ++t, ++wq) {
+                  const int s = wq % kWStages;
+                  const uint32_t u = wq / kWStages;
+                  if (u > 0 && !(ok = wait_bar(&bars->w_empty[s], (u - 1) & 1, abort_flag, p.err))) break;
+                  mbar_expect_tx(&bars->w_full[s], (uint32_t)box[jb] * BK * 2);
+                  tma_load_2d(t ? wml[jb] : wm[jb], &bars->w_full[s], wring + s * kWStage, kc * BK,
+                              g * rows_g[jb] + c * 256);
+                }
               }
             }
           }
@@ -230,9 +269,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
       // Before the CTA can exit, every issued TMA load must have landed (on an
       // abort some stages may never be consumed).  Bounded, ignores the abort flag.
       int dummy = 0;
-      for (uint32_t s = 0; s < (uint32_t)kXStages && s < xq; ++s) {
-        const uint32_t last = xq - 1 - ((xq - 1 - s) % kXStages);
-        wait_bar(&bars->x_full[s], (last / kXStages) & 1, &dummy, p.err);
+      for (uint32_t s = 0; s < (uint32_t)XS && s < xq; ++s) {
+        const uint32_t last = xq - 1 - ((xq - 1 - s) % XS);
+        wait_bar(&bars->x_full[s], (last / XS) & 1, &dummy, p.err);
       }
       for (uint32_t s = 0; s < (uint32_t)kWStages && s < wq; ++s) {
         const uint32_t last = wq - 1 - ((wq - 1 - s) % kWStages);
@@ -255,25 +294,38 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
       // one GEMM whose A operand is the activation buffer (K/64 atoms) and B the
       // weight ring.  With wait_act, each K-atom is used as soon as the epilogue
       // has published it, so the GEMM overlaps the epilogue that feeds it.
-      auto gemm_act = [&](int n, int k, uint32_t b, bool wait_act) -> bool {
-        const uint32_t idesc = idesc_bf16_f32(n);
+      // alo: A carries a lo part; wlo: each K step also has a W lo chunk.
+      auto gemm_act = [&](int n, int k, uint32_t b, bool wait_act, bool alo, bool wlo) -> bool {
+        const uint32_t idesc = F16 ? idesc_f16_f32(n) : idesc_bf16_f32(n);
         const uint32_t d = tmem + b * 256;
-        for (int kc = 0; kc < k / BK; ++kc, ++wq) {
+        for (int kc = 0; kc < k / BK; ++kc) {
           if (wait_act) {
             if (!wait_bar(&bars->act_ready[kc], act_phase[kc] & 1, abort_flag, p.err)) return false;
             ++act_phase[kc];
           }
-          const int s = wq % kWStages;
+          int s = wq % kWStages;
           if (!wait_bar(&bars->w_full[s], (wq / kWStages) & 1, abort_flag, p.err)) return false;
           fence_after_sync();
-          const uint32_t bs = smem_u32(wring + s * kWStage);
+          uint32_t bs = smem_u32(wring + s * kWStage);
 #pragma unroll
           for (int kk = 0; kk < BK / 16; ++kk) {
             const uint64_t bd = sdesc_sw128(bs + kk * 32);
             mma_bf16(d, sdesc_sw128(act_hi + kc * kAtom + kk * 32), bd, idesc, (kc | kk) != 0);
-            if (p.a_lo) mma_bf16(d, sdesc_sw128(act_lo + kc * kAtom + kk * 32), bd, idesc, 1u);
+            if (alo) mma_bf16(d, sdesc_sw128(act_lo + kc * kAtom + kk * 32), bd, idesc, 1u);
           }
           mma_commit(&bars->w_empty[s]);
+          ++wq;
+          if (wlo) {
+            s = wq % kWStages;
+            if (!wait_bar(&bars->w_full[s], (wq / kWStages) & 1, abort_flag, p.err)) return false;
+            fence_after_sync();
+            bs = smem_u32(wring + s * kWStage);
+#pragma unroll
+            for (int kk = 0; kk < BK / 16; ++kk)
+              mma_bf16(d, sdesc_sw128(act_hi + kc * kAtom + kk * 32), sdesc_sw128(bs + kk * 32), idesc, 1u);
+            mma_commit(&bars->w_empty[s]);
+            ++wq;
+          }
         }
         return true;
       };
@@ -283,18 +335,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
           {
             const uint32_t b = job & 1;
             if (!(ok = acquire_acc(b))) break;
-            const uint32_t idesc = idesc_bf16_f32(p.d1);
+            const uint32_t idesc = F16 ? idesc_f16_f32(p.d1) : idesc_bf16_f32(p.d1);
             const uint32_t d = tmem + b * 256;
             for (int kc = 0; kc < p.d0 / BK; ++kc, ++xq) {
-              const int s = xq % kXStages;
-              if (!(ok = wait_bar(&bars->x_full[s], (xq / kXStages) & 1, abort_flag, p.err))) break;
+              const int s = xq % XS;
+              if (!(ok = wait_bar(&bars->x_full[s], (xq / XS) & 1, abort_flag, p.err))) break;
               fence_after_sync();
-              const uint32_t st = smem_u32(act + s * kXStage);
+              const uint32_t st = smem_u32(act + s * p.xstage);
 #pragma unroll
               for (int kk = 0; kk < BK / 16; ++kk) {
+                const uint64_t ad = sdesc_sw128(st + kk * 32);
                 const uint64_t bd = sdesc_sw128(st + 2 * kAtom + kk * 32);
-                mma_bf16(d, sdesc_sw128(st + kk * 32), bd, idesc, (kc | kk) != 0);
+                mma_bf16(d, ad, bd, idesc, (kc | kk) != 0);
                 if (p.a_lo) mma_bf16(d, sdesc_sw128(st + kAtom + kk * 32), bd, idesc, 1u);
+                if (p.wf_lo) mma_bf16(d, ad, sdesc_sw128(st + 4 * kAtom + kk * 32), idesc, 1u);
               }
               mma_commit(&bars->x_empty[s]);
             }
@@ -308,8 +362,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
           const int ks[4] = {p.d1, p.d2, p.d3, p.d2};
           for (int jb = 0; jb < 4 && ok; ++jb) {
             const uint32_t b = job & 1;
+            const bool fwd = jb < 2;
             if (!(ok = acquire_acc(b))) break;
-            if (!(ok = gemm_act(ns[jb], ks[jb], b, true))) break;
+            if (!(ok = gemm_act(ns[jb], ks[jb], b, true, fwd ? p.a_lo : p.g_lo, fwd ? p.wf_lo : p.wb_lo))) break;
             mma_commit(&bars->acc_full[b]);
             ++nuse[b];
             ++job;
@@ -319,7 +374,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
           for (int c = 0; c < p.d0 / 256 && ok; ++c) {
             const uint32_t b = job & 1;
             if (!(ok = acquire_acc(b))) break;
-            if (!(ok = gemm_act(256, p.d1, b, c == 0))) break;
+            if (!(ok = gemm_act(256, p.d1, b, c == 0, p.g_lo, p.wb_lo))) break;
             mma_commit(&bars->acc_full[b]);
             ++nuse[b];
             ++job;
@@ -344,7 +399,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
     // per-CTA CELU' scratch, column-major [d1 + d2][128] so that a warp's 32 rows are contiguous
     float* dc = p.dc + (size_t)blockIdx.x * BM * (p.d1 + p.d2) + r;
     const float inv_alpha = 1.0f / p.alpha;
-    const bool with_lo = p.a_lo != 0;
+    const bool with_lo = p.a_lo != 0;    // forward activations
+    const bool grad_lo = p.g_lo != 0;    // input-gradient operands
     auto take_acc = [&](uint32_t b) -> bool {
       bool ready = __all_sync(0xffffffffu, wait_bar(&bars->acc_full[b], nuse[b] & 1, abort_flag, p.err));
       if (ready) fence_after_sync();
@@ -363,10 +419,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
       fence_proxy_async();
       mbar_arrive(&bars->act_ready[a]);
     };
-    // H = celu(Z + bias) -> act for columns [0, n); celu'(z) -> dc columns
+    // H = celu(Z / s_W + bias) -> act for columns [0, n); celu'(z) -> dc columns
     // [dc0, dc0 + n).  The bias loads are issued before the TMEM load so that
-    // their latencies overlap.
-    auto celu_layer = [&](uint32_t b, const float* bias, int n, int dc0) {
+    // their latencies overlap.  inv_s = 1 / s_W (1 for the BF16 forms).
+    auto celu_layer = [&](uint32_t b, const float* bias, int n, int dc0, float inv_s) {
       for (int cc = half; cc < n / 32; cc += 2) {
         float4 bb[8];
 #pragma unroll
@@ -376,8 +432,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
         float* dco = dc + (size_t)(dc0 + cc * 32) * BM;
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
-          const float zz[4] = {v[4 * k] + bb[k].x, v[4 * k + 1] + bb[k].y, v[4 * k + 2] + bb[k].z,
-                               v[4 * k + 3] + bb[k].w};
+          const float zz[4] = {fmaf(v[4 * k], inv_s, bb[k].x), fmaf(v[4 * k + 1], inv_s, bb[k].y),
+                               fmaf(v[4 * k + 2], inv_s, bb[k].z), fmaf(v[4 * k + 3], inv_s, bb[k].w)};
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
             float dh;
@@ -385,14 +441,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
             dco[(size_t)(4 * k + u) * BM] = dh;  // column-major: the warp writes 128 contiguous bytes
           }
         }
-        act_store(act, r, cc * 32, v, with_lo);
+        act_store<F16>(act, r, cc * 32, v, with_lo);
         publish_atom(cc >> 1);
       }
     };
-    // G = D * celu'(z) -> act for columns [0, n), celu' read back from dc
+    // G = D / s_W * celu'(z) -> act for columns [0, n), celu' read back from dc
     // columns [dc0, dc0 + n) (written by this thread); loads issued before the
     // TMEM load.
-    auto mask_layer = [&](uint32_t b, int n, int dc0) {
+    auto mask_layer = [&](uint32_t b, int n, int dc0, float inv_s) {
       for (int cc = half; cc < n / 32; cc += 2) {
         const float* dci = dc + (size_t)(dc0 + cc * 32) * BM;
         float dd[32];
@@ -401,8 +457,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
         float v[32];
         tmem_ld32(tmem + b * 256 + lane_base + cc * 32, v);
 #pragma unroll
-        for (int k = 0; k < 32; ++k) v[k] *= dd[k];
-        act_store(act, r, cc * 32, v, with_lo);
+        for (int k = 0; k < 32; ++k) v[k] = (v[k] * inv_s) * dd[k];
+        act_store<F16>(act, r, cc * 32, v, grad_lo);
         publish_atom(cc >> 1);
       }
     };
@@ -412,21 +468,30 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
       float e_row = 0.f;  // ensemble-mean row energy, accumulated model by model in registers
       for (int m = 0; m < M && ok; ++m) {
         const int g = m * p.n_species + sp;
+        // weight scales of this group (powers of two: the reciprocals are exact)
+        float inv_s1 = 1.f, inv_s2 = 1.f, inv_s3 = 1.f, s_g = 1.f;
+        if constexpr (F16) {
+          const float4 sc = __ldg(p.scales + g);
+          inv_s1 = 1.f / sc.x;
+          inv_s2 = 1.f / sc.y;
+          inv_s3 = 1.f / sc.z;
+          s_g = sc.w;
+        }
         // E1: H1 = celu(Z1 + b1) -> act; celu'(z1) -> dc[0:d1]
         {
           const uint32_t b = job & 1;
           if (!(ok = take_acc(b))) break;
-          celu_layer(b, p.b1 + (size_t)g * p.d1, p.d1, 0);
+          celu_layer(b, p.b1 + (size_t)g * p.d1, p.d1, 0, inv_s1);
           release_acc(b);
         }
         // E2: H2 = celu(Z2 + b2) -> act; celu'(z2) -> dc[d1:d1+d2]
         {
           const uint32_t b = job & 1;
           if (!(ok = take_acc(b))) break;
-          celu_layer(b, p.b2 + (size_t)g * p.d2, p.d2, p.d1);
+          celu_layer(b, p.b2 + (size_t)g * p.d2, p.d2, p.d1, inv_s2);
           release_acc(b);
         }
-        // E3: energy head; G3 = w4 * celu'(z3) -> act.  Both column halves work;
+        // E3: energy head; G3 = s_g w4 * celu'(z3) -> act.  Both column halves work;
         // the half-1 partial energy of each row reaches the half-0 thread through
         // shared memory guarded by two mbarriers (bounded waits, no CTA barrier).
         {
@@ -446,18 +511,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
             tmem_ld32(tmem + b * 256 + lane_base + cc * 32, v);
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
-              const float zz[4] = {v[4 * k] + bb[k].x, v[4 * k + 1] + bb[k].y, v[4 * k + 2] + bb[k].z,
-                                   v[4 * k + 3] + bb[k].w};
+              const float zz[4] = {fmaf(v[4 * k], inv_s3, bb[k].x), fmaf(v[4 * k + 1], inv_s3, bb[k].y),
+                                   fmaf(v[4 * k + 2], inv_s3, bb[k].z), fmaf(v[4 * k + 3], inv_s3, bb[k].w)};
               const float wv[4] = {ww[k].x, ww[k].y, ww[k].z, ww[k].w};
 #pragma unroll
               for (int u = 0; u < 4; ++u) {
                 float h, dh;
                 celu_pair(zz[u], p.alpha, inv_alpha, h, dh);
                 e = fmaf(h, wv[u], e);
-                v[4 * k + u] = wv[u] * dh;
+                v[4 * k + u] = (s_g * wv[u]) * dh;
               }
             }
-            act_store(act, r, cc * 32, v, with_lo);
+            act_store<F16>(act, r, cc * 32, v, grad_lo);
             publish_atom(cc >> 1);
           }
           release_acc(b);
@@ -479,14 +544,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
         {
           const uint32_t b = job & 1;
           if (!(ok = take_acc(b))) break;
-          mask_layer(b, p.d2, p.d1);
+          mask_layer(b, p.d2, p.d1, inv_s3);
           release_acc(b);
         }
         // E5: G1 = D1 * celu'(z1) -> act
         {
           const uint32_t b = job & 1;
           if (!(ok = take_acc(b))) break;
-          mask_layer(b, p.d1, 0);
+          mask_layer(b, p.d1, 0, inv_s2);
           release_acc(b);
         }
         // E6: dX chunks.  Each warp stages a 32 x 32 block (its 32 rows, 32
@@ -501,6 +566,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
         uint8_t* tile = reinterpret_cast<uint8_t*>(xpose + (warp - 2) * 32 * 32);
         uint8_t* trow = tile + lane * 128;
         const int dx_row = p.tile_row[w] + 32 * q;
+        const float dx_scale = p.inv_models * (inv_s1 / s_g);
         for (int c = 0; c < p.d0 / 256 && ok; ++c) {
           const uint32_t b = job & 1;
           if (!(ok = take_acc(b))) break;
@@ -512,8 +578,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
 #pragma unroll
             for (int j = 0; j < 8; ++j)
               *reinterpret_cast<float4*>(trow + ((j ^ (lane & 7)) << 4)) =
-                  make_float4(v[4 * j] * p.inv_models, v[4 * j + 1] * p.inv_models, v[4 * j + 2] * p.inv_models,
-                              v[4 * j + 3] * p.inv_models);
+                  make_float4(v[4 * j] * dx_scale, v[4 * j + 1] * dx_scale, v[4 * j + 2] * dx_scale,
+                              v[4 * j + 3] * dx_scale);
             fence_proxy_async();
             __syncwarp();
             if (lane == 0) {
@@ -555,14 +621,16 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-bool map2d(CUtensorMap* m, const void* base, uint64_t rows, uint64_t cols, uint32_t box_rows) {
+// 16-bit [rows][cols] operand (BF16, or FP16 when f16) in BK x box_rows boxes
+bool map2d(CUtensorMap* m, const void* base, uint64_t rows, uint64_t cols, uint32_t box_rows, bool f16 = false) {
   auto fn = encode_fn();
   if (!fn || !base) return false;
   cuuint64_t dims[2] = {cols, rows};
   cuuint64_t strides[1] = {cols * 2};
   cuuint32_t box[2] = {(cuuint32_t)BK, box_rows};
   cuuint32_t estr[2] = {1, 1};
-  return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+  return fn(m, f16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base),
+            dims, strides, box, estr,
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
@@ -590,13 +658,18 @@ int sm_count() {
   return n;
 }
 
+bool is_f16_form(int precision) {
+  return precision == FENNOL_MLP_F16X3X1 || precision == FENNOL_MLP_F16X3X2;
+}
+
 }  // namespace
 
 // Shape check: the fused kernel needs every hidden width <= 256 (activation
-// buffer), the input width a multiple of 256 and a BF16 or BF16x2 product.
+// buffer), the input width a multiple of 256 and a BF16, BF16x2 or FP16 form.
 bool fnl_mlp_fused_supported(int precision, const fennol_mlp_weights* w) {
   const int* d = w->dims;
-  if (precision != FENNOL_MLP_BF16 && precision != FENNOL_MLP_BF16X2) return false;
+  if (precision != FENNOL_MLP_BF16 && precision != FENNOL_MLP_BF16X2 && !is_f16_form(precision)) return false;
+  if (is_f16_form(precision) && !w->f16_scale) return false;
   if (d[0] % 256 != 0 || d[0] > 4096) return false;
   for (int l = 1; l < 4; ++l)
     if (d[l] > 256 || d[l] % 64 != 0) return false;
@@ -614,15 +687,33 @@ int fnl_mlp_fused(int precision, int rows, int ntiles, const int* tile_species, 
   if (ws_bytes < fnl_mlp_fused_workspace(w)) return FENNOL_ERR_WORKSPACE;
   const int* d = w->dims;
   const int G = w->n_models * w->n_species;
-  const bool alo = precision == FENNOL_MLP_BF16X2;
+  const bool f16 = is_f16_form(precision);
+  const bool alo = precision == FENNOL_MLP_BF16X2 || f16;
+  const bool glo = precision == FENNOL_MLP_BF16X2;
+  const bool wflo = f16;
+  const bool wblo = precision == FENNOL_MLP_F16X3X2;
+  if (f16 && (!w->wt_lo[0] || !w->wt_lo[1] || !w->wt_lo[2])) return FENNOL_ERR_INVALID;
+  if (wblo && (!w->w_lo[0] || !w->w_lo[1] || !w->w_lo[2])) return FENNOL_ERR_INVALID;
+  if (f16 && ((uintptr_t)w->f16_scale & 15) != 0) return FENNOL_ERR_INVALID;
+  // maps of absent low parts alias the high parts (never loaded)
+  const void* wtl[3] = {wflo ? w->wt_lo[0] : w->wt_hi[0], wflo ? w->wt_lo[1] : w->wt_hi[1],
+                        wflo ? w->wt_lo[2] : w->wt_hi[2]};
+  const void* wl[3] = {wblo ? w->w_lo[0] : w->w_hi[0], wblo ? w->w_lo[1] : w->w_hi[1],
+                       wblo ? w->w_lo[2] : w->w_hi[2]};
   Maps maps;
-  bool ok = map2d(&maps.x, x, rows, d[0], BM) && map2d(&maps.xlo, alo ? x_lo : x, rows, d[0], BM) &&
-            map2d(&maps.w1t, w->wt_hi[0], (uint64_t)G * d[1], d[0], d[1]) &&
-            map2d(&maps.w2t, w->wt_hi[1], (uint64_t)G * d[2], d[1], d[2]) &&
-            map2d(&maps.w3t, w->wt_hi[2], (uint64_t)G * d[3], d[2], d[3]) &&
-            map2d(&maps.w3, w->w_hi[2], (uint64_t)G * d[2], d[3], d[2]) &&
-            map2d(&maps.w2, w->w_hi[1], (uint64_t)G * d[1], d[2], d[1]) &&
-            map2d(&maps.w1, w->w_hi[0], (uint64_t)G * d[0], d[1], 256) && map_dx(&maps.dx, dx, rows, d[0]);
+  bool ok = map2d(&maps.x, x, rows, d[0], BM, f16) && map2d(&maps.xlo, alo ? x_lo : x, rows, d[0], BM, f16) &&
+            map2d(&maps.w1t, w->wt_hi[0], (uint64_t)G * d[1], d[0], d[1], f16) &&
+            map2d(&maps.w2t, w->wt_hi[1], (uint64_t)G * d[2], d[1], d[2], f16) &&
+            map2d(&maps.w3t, w->wt_hi[2], (uint64_t)G * d[3], d[2], d[3], f16) &&
+            map2d(&maps.w3, w->w_hi[2], (uint64_t)G * d[2], d[3], d[2], f16) &&
+            map2d(&maps.w2, w->w_hi[1], (uint64_t)G * d[1], d[2], d[1], f16) &&
+            map2d(&maps.w1, w->w_hi[0], (uint64_t)G * d[0], d[1], 256, f16) &&
+            map2d(&maps.w1t_lo, wtl[0], (uint64_t)G * d[1], d[0], d[1], f16) &&
+            map2d(&maps.w2t_lo, wtl[1], (uint64_t)G * d[2], d[1], d[2], f16) &&
+            map2d(&maps.w3t_lo, wtl[2], (uint64_t)G * d[3], d[2], d[3], f16) &&
+            map2d(&maps.w3_lo, wl[2], (uint64_t)G * d[2], d[3], d[2], f16) &&
+            map2d(&maps.w2_lo, wl[1], (uint64_t)G * d[1], d[2], d[1], f16) &&
+            map2d(&maps.w1_lo, wl[0], (uint64_t)G * d[0], d[1], 256, f16) && map_dx(&maps.dx, dx, rows, d[0]);
   if (!ok) return FENNOL_ERR_CUDA;
   FusedParams p{};
   p.ntiles = ntiles;
@@ -635,6 +726,12 @@ int fnl_mlp_fused(int precision, int rows, int ntiles, const int* tile_species, 
   p.d2 = d[2];
   p.d3 = d[3];
   p.a_lo = alo ? 1 : 0;
+  p.g_lo = glo ? 1 : 0;
+  p.wf_lo = wflo ? 1 : 0;
+  p.wb_lo = wblo ? 1 : 0;
+  p.xstages = wflo ? kXStagesWide : kXStages;
+  p.xstage = wflo ? kXStageWide : kXStage;
+  p.scales = reinterpret_cast<const float4*>(w->f16_scale);
   p.alpha = w->celu_alpha;
   p.inv_models = 1.0f / (float)w->n_models;
   p.b1 = w->b32[0];
@@ -647,15 +744,16 @@ int fnl_mlp_fused(int precision, int rows, int ntiles, const int* tile_species, 
   p.err = (int*)ws;
   p.dc = (float*)((char*)ws + 256);
   const size_t smem = kSmemMain + sizeof(Bars) + 1024;
-  static bool attr = false;
-  if (!attr) {
-    if (cudaFuncSetAttribute(k_mlp_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+  static bool attr[2] = {false, false};
+  auto kern = f16 ? k_mlp_fused<true> : k_mlp_fused<false>;
+  if (!attr[f16]) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
       return FENNOL_ERR_CUDA;
-    attr = true;
+    attr[f16] = true;
   }
   if (ntiles <= 0) return FENNOL_OK;
   const int grid = ntiles < sm_count() ? ntiles : sm_count();
-  FNL_LAUNCH_PDL(k_mlp_fused, dim3(grid), dim3(kThreads), smem, st, maps, p);
+  FNL_LAUNCH_PDL(kern, dim3(grid), dim3(kThreads), smem, st, maps, p);
   FNL_CHECK_LAUNCH();
   return FENNOL_OK;
 }

@@ -469,8 +469,10 @@ int fnl_mlp_tc(int precision, int rows, int ntiles, const int* tile_species, con
                const fennol_mlp_weights* w, const void* x, const void* x_lo, float* e_rows, float* dx, void* ws,
                size_t ws_bytes, cudaStream_t st) {
   if (!encode_fn()) return FENNOL_ERR_UNSUPPORTED;
-  if (fnl_mlp_fused_supported(precision, w) && !getenv("FENNOL_MLP_UNFUSED"))
+  const bool f16 = precision == FENNOL_MLP_F16X3X1 || precision == FENNOL_MLP_F16X3X2;
+  if (fnl_mlp_fused_supported(precision, w) && (f16 || !getenv("FENNOL_MLP_UNFUSED")))
     return fnl_mlp_fused(precision, rows, ntiles, tile_species, tile_row, w, x, x_lo, e_rows, dx, ws, ws_bytes, st);
+  if (f16) return FENNOL_ERR_UNSUPPORTED;  // the FP16 forms exist only as the fused kernel
   const int* d = w->dims;
   for (int l = 0; l < 4; ++l)
     if (d[l] > 1024 || (l > 0 && d[l] > 256)) return FENNOL_ERR_UNSUPPORTED;

@@ -138,6 +138,11 @@ __device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr) {
 __host__ __device__ constexpr uint32_t idesc_bf16_f32(int n) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
 }
+// kind::f16 instruction descriptor: FP16 x FP16 -> F32 (A and B type fields 0),
+// both K-major, M = 128.
+__host__ __device__ constexpr uint32_t idesc_f16_f32(int n) {
+  return (1u << 4) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
 
 __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
                                          uint32_t accumulate) {

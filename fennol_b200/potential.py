@@ -57,9 +57,28 @@ def round_weights_bf16(weights: Weights) -> Weights:
     return out
 
 
+def pow2_scale(a: np.ndarray) -> float:
+    """The power of two that brings the largest |a| into [1, 2) (1 for zeros)."""
+    m = float(np.max(np.abs(a))) if a.size else 0.0
+    return 1.0 if m == 0.0 else float(2.0 ** (-math.floor(math.log2(m))))
+
+
+def split16(W: torch.Tensor, dtype) -> Tuple[torch.Tensor, torch.Tensor]:
+    """W (float64) as hi + lo of a 16-bit type, each rounded to nearest."""
+    hi = W.to(dtype)
+    lo = (W - hi.to(torch.float64)).to(dtype)
+    return hi, lo
+
+
 class PackedMLP:
     """Device copies of the species networks in the layouts the kernels read
-    (see ``fennol_mlp_weights`` in ``include/fennol_b200.h``)."""
+    (see ``fennol_mlp_weights`` in ``include/fennol_b200.h``).
+
+    The FP16 forms store every kernel of layers 1-3 multiplied by a power of
+    two per (model, species) group that puts its largest entry in [1, 2), so
+    that the float16 hi + lo split keeps about 22 bits of each weight; the
+    scales go to the kernel in ``f16_scale`` together with the power of two
+    applied to the last layer inside the input-gradient GEMMs."""
 
     def __init__(self, weights: Weights, aev: AEVConfig, mlp: MLPConfig, device, precision: int):
         self.n_models = len(weights)
@@ -70,6 +89,9 @@ class PackedMLP:
         dims = [_ceil(d, 64) for d in real[:-1]] + [1]
         self.real_dims, self.dims = real, dims
         G = self.n_models * self.n_species
+        f16 = precision in _lib.F16_FORMS
+        half = torch.float16 if f16 else torch.bfloat16
+        scales = np.ones((G, 4))
         w32, b32, wt_hi, wt_lo, w_hi, w_lo = [], [], [], [], [], []
         for l in range(4):
             W = np.zeros((G, dims[l], dims[l + 1]))
@@ -85,15 +107,21 @@ class PackedMLP:
             Wt = torch.tensor(W, dtype=torch.float64)
             w32.append(Wt.to(torch.float32).to(device).contiguous())
             b32.append(torch.tensor(B, dtype=torch.float32, device=device).contiguous())
+            if f16:
+                # scales of the float32 kernel the other forms evaluate
+                W32 = W.astype(np.float32).astype(np.float64)
+                for g in range(G):
+                    scales[g, l] = pow2_scale(W32[g])
+                Wt = torch.tensor(W32 * scales[:, l][:, None, None], dtype=torch.float64)
             if precision != _lib.MLP_FP32 and l < 3:
-                hi = Wt.to(torch.bfloat16)
-                lo = (Wt - hi.to(torch.float64)).to(torch.bfloat16)
+                hi, lo = split16(Wt, half)
                 w_hi.append(hi.to(device).contiguous())
                 w_lo.append(lo.to(device).contiguous())
                 wt_hi.append(hi.transpose(1, 2).contiguous().to(device))
                 wt_lo.append(lo.transpose(1, 2).contiguous().to(device))
             else:
                 w_hi.append(None), w_lo.append(None), wt_hi.append(None), wt_lo.append(None)
+        self.scales = (torch.tensor(scales, dtype=torch.float32, device=device).contiguous() if f16 else None)
         self._keep = (w32, b32, wt_hi, wt_lo, w_hi, w_lo)
         s = _lib.MLPWeights()
         s.n_models = self.n_models
@@ -108,6 +136,7 @@ class PackedMLP:
             s.wt_lo[l] = _ptr(wt_lo[l])
             s.w_hi[l] = _ptr(w_hi[l])
             s.w_lo[l] = _ptr(w_lo[l])
+        s.f16_scale = _ptr(self.scales)
         self.struct = s
 
 
@@ -316,6 +345,10 @@ class Workspace:
             self.x = torch.zeros((rows, d0), dtype=torch.float32, device=dev)
             self.x_lo = None
             self.aev_kind = _lib.AEV_F32
+        elif pot.precision in _lib.F16_FORMS:
+            self.x = torch.zeros((rows, d0), dtype=torch.float16, device=dev)
+            self.x_lo = torch.zeros((rows, d0), dtype=torch.float16, device=dev)
+            self.aev_kind = _lib.AEV_F16X2
         else:
             self.x = torch.zeros((rows, d0), dtype=torch.bfloat16, device=dev)
             self.x_lo = (torch.zeros((rows, d0), dtype=torch.bfloat16, device=dev)
@@ -349,7 +382,11 @@ class ANIPotential:
     """ANI-2x-style potential evaluated by the sm_100a kernels.
 
     ``precision``: ``"fp32"`` (CUDA-core GEMMs), ``"bf16"``, ``"bf16x2"`` or
-    ``"bf16x3"`` (tcgen05 tensor-core GEMMs with 1, 2 or 3 BF16 products).
+    ``"bf16x3"`` (tcgen05 tensor-core GEMMs with 1, 2 or 3 BF16 products), or
+    ``"f16x3x1"`` / ``"f16x3x2"`` (tcgen05 FP16 hi + lo splits of activations
+    and scaled float32 weights: 3 products in the forward GEMMs, 1 or 2 in the
+    input-gradient GEMMs; within the energy and force budgets against the
+    FP64 model for float32 weights).
     ``bf16_weights`` rounds the kernels to BFloat16 (a model stored in BF16);
     bf16x2 is exact in the weights for such a model.
     ``minimum_image``: True / False force the minimum-image or the general
@@ -432,6 +469,8 @@ class ANIPotential:
         import os
         if self.precision == _lib.MLP_FP32:
             return 7 * self.mlp.n_models
+        if self.precision in _lib.F16_FORMS:
+            return 1
         fused = (self.precision in (_lib.MLP_BF16, _lib.MLP_BF16X2) and self.mlp.dims[0] % 256 == 0
                  and max(self.mlp.dims[1:4]) <= 256 and not os.environ.get("FENNOL_MLP_UNFUSED"))
         return 1 if fused else 6 * self.mlp.n_models + 1

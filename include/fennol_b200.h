@@ -183,6 +183,7 @@ int fennol_pack_atoms(const float* coords, const int* species_idx, int natoms, f
 #define FENNOL_AEV_F32 0     /* float32 rows */
 #define FENNOL_AEV_BF16 1    /* bfloat16 rows */
 #define FENNOL_AEV_BF16X2 2  /* bfloat16 hi rows + bfloat16 lo rows (x ~= hi + lo) */
+#define FENNOL_AEV_F16X2 3   /* float16 hi rows + float16 lo rows (x ~= hi + lo, ~22 bits) */
 
 /*
  * ANIAEV forward.  Replaces ANIAEV.__call__ (embeddings/ani.py:47-142) with
@@ -275,6 +276,12 @@ int fennol_aev_tangent(const float* xyzs, int natoms, const int* atom_sys, const
 #define FENNOL_MLP_BF16 1     /* tcgen05 BF16 x BF16, FP32 accumulate */
 #define FENNOL_MLP_BF16X2 2   /* activations split hi+lo BF16 (2 MMAs); weights as BF16 */
 #define FENNOL_MLP_BF16X3 3   /* activations and weights split (3 MMAs) */
+/* FP16 forms for float32 weights: activations and power-of-two-scaled weights
+ * split into float16 hi + lo (about 22 bits each).  The forward GEMMs take
+ * three products (A_hi W_hi + A_lo W_hi + A_hi W_lo); the input-gradient GEMMs
+ * take one (G_hi W_hi, F16X3X1) or two (G_hi W_hi + G_hi W_lo, F16X3X2). */
+#define FENNOL_MLP_F16X3X1 4
+#define FENNOL_MLP_F16X3X2 5
 
 #define FENNOL_MLP_LAYERS 4
 
@@ -291,6 +298,12 @@ int fennol_aev_tangent(const float* xyzs, int natoms, const int* atom_sys, const
  *                        input-gradient GEMMs); used for l = 0..2.
  * bf16 pointers may be NULL for FENNOL_MLP_FP32; *_lo may be NULL unless
  * FENNOL_MLP_BF16X3.
+ * For FENNOL_MLP_F16X3X1 / F16X3X2 the four split copies are float16 and hold
+ * kernel * f16_scale[g*4 + l] (l = 0..2), a power of two chosen per group and
+ * layer so that the largest entry lies in [1, 2); f16_scale[g*4 + 3] is the
+ * power of two applied to the last layer's kernel inside the input-gradient
+ * GEMMs.  wt_lo is required for both FP16 forms, w_lo for F16X3X2 only.
+ * f16_scale (16-byte aligned) may be NULL for the other forms.
  */
 typedef struct fennol_mlp_weights {
   int n_models;
@@ -303,6 +316,7 @@ typedef struct fennol_mlp_weights {
   const void* wt_lo[FENNOL_MLP_LAYERS];
   const void* w_hi[FENNOL_MLP_LAYERS];
   const void* w_lo[FENNOL_MLP_LAYERS];
+  const float* f16_scale;
 } fennol_mlp_weights;
 
 /* Workspace of fennol_mlp_energy_grad for `rows` padded rows, in bytes. */
@@ -315,7 +329,9 @@ size_t fennol_mlp_workspace_bytes(int precision, int rows, int n_models,
  * ensemble mean.  Rows are grouped by species in tiles of 128: tile t covers
  * rows [tile_row[t], tile_row[t]+128) of species tile_species[t] (padding
  * rows must hold zeros).  Inputs: x (AEV rows, ld = dims[0]; float32 for
- * FENNOL_MLP_FP32, bfloat16 hi (+ lo) otherwise).  Outputs: e_rows[rows]
+ * FENNOL_MLP_FP32, float16 hi + lo for the FP16 forms, bfloat16 hi (+ lo)
+ * otherwise).  The FP16 forms run only as the fused kernel (hidden widths
+ * <= 256, input width a multiple of 256; FENNOL_ERR_UNSUPPORTED otherwise).  Outputs: e_rows[rows]
  * (ensemble-mean atomic energy) and dx[rows*dims[0]] (float32 dE/dAEV,
  * ensemble mean).
  */

@@ -2,10 +2,12 @@
 and the FP32 CUDA-core form.
 
 Tolerances: force RMSE <= 0.05 kcal/mol/A and |dE|/N <= 1e-4 kcal/mol/atom
-for bf16x2 on BF16-exact weights (the BF16 model form); bf16x3 on arbitrary
-float weights carries a systematic ~1e-4 kcal/mol/atom energy bias from the
-weights' own hi+lo representation and is held to 3e-4; the single-product
-BF16 form is reported against a looser bound."""
+(max over systems) against the FP64 oracle of the same float32 weights for
+the FP16 forms f16x3x1 / f16x3x2 (seeded N(0, 1/fan_in) weights, not
+rounded), and for bf16x2 on BF16-exact weights (the BF16 model form).
+bf16x3 on arbitrary float weights carries a systematic ~1e-4 kcal/mol/atom
+energy bias from the weights' own 16-bit hi+lo representation and is held to
+3e-4; the single-product BF16 form is reported against a looser bound."""
 
 import numpy as np
 import pytest
@@ -88,3 +90,75 @@ def test_tensor_core_matches_fp32_form(cuda_device):
     assert abs(float(e32[0]) - float(etc[0])) * HARTREE_TO_KCALMOL / s.natoms < 3e-4
     rmse = float(torch.sqrt(torch.mean((f32 - ftc) ** 2))) * HARTREE_TO_KCALMOL
     assert rmse < 0.05
+
+
+# ---- FP16 split forms on the unrounded float32 model --------------------------------
+
+E_BUDGET, F_BUDGET = 1e-4, 0.05   # kcal/mol/atom, kcal/mol/A
+
+
+@pytest.mark.parametrize("precision", ["f16x3x1", "f16x3x2"])
+def test_f16_forms_water64_unrounded(cuda_device, precision):
+    """C1: 64 waters, one model with the seeded float32 weights."""
+    pot = ANIPotential(precision=precision, device=cuda_device, seed=0)
+    s = water_box(4, seed=0)
+    de, rmse = errors(pot, s.coordinates, s.species, [s.natoms], s.cell[None])
+    assert _err_word(pot) == 0
+    assert de <= E_BUDGET and rmse <= F_BUDGET, (de, rmse)
+    if precision == "f16x3x2":
+        assert rmse <= 0.03, rmse   # the two-product input gradient: ~0.02 expected
+
+
+@pytest.mark.parametrize("precision", ["f16x3x1", "f16x3x2"])
+def test_f16_forms_water12k_unrounded(cuda_device, precision):
+    """The 12,288-atom water box (4096 H2O), one model, float32 weights."""
+    pot = ANIPotential(precision=precision, device=cuda_device, seed=0)
+    s = water_box(16, seed=1)
+    de, rmse = errors(pot, s.coordinates, s.species, [s.natoms], s.cell[None])
+    assert _err_word(pot) == 0
+    assert de <= E_BUDGET and rmse <= F_BUDGET, (de, rmse)
+
+
+def test_f16x3x1_ensemble8_unrounded(cuda_device):
+    """8-model ensemble (independent seeds) on a 1536-atom water box."""
+    W = init_weights(CFG, MCFG, seed=0, n_models=8)
+    pot = ANIPotential(precision="f16x3x1", device=cuda_device, weights=W)
+    s = water_box(8, seed=2)
+    de, rmse = errors(pot, s.coordinates, s.species, [s.natoms], s.cell[None])
+    assert _err_word(pot) == 0
+    assert de <= E_BUDGET and rmse <= F_BUDGET, (de, rmse)
+
+
+@pytest.mark.parametrize("precision", ["f16x3x1", "f16x3x2"])
+def test_f16_forms_molecules_all_species(cuda_device, precision):
+    """30 molecules of 10-40 atoms with all seven species, 3-model ensemble:
+    small systems, so the per-atom energy error is the max over molecules."""
+    W = init_weights(CFG, MCFG, seed=5, n_models=3)
+    pot = ANIPotential(precision=precision, device=cuda_device, weights=W)
+    mols = molecule_batch(30, seed=8)
+    xyz = np.concatenate([m.coordinates for m in mols])
+    sp = np.concatenate([m.species for m in mols])
+    nat = [m.natoms for m in mols]
+    de, rmse = errors(pot, xyz, sp, nat)
+    assert de <= E_BUDGET and rmse <= F_BUDGET, (de, rmse)
+
+
+def test_f16_form_md_scale_model(cuda_device):
+    """The MD workloads' model (last layer x 0.02): small weights in the last
+    layer exercise the power-of-two gradient scale."""
+    from fennol_b200.params import MD_OUTPUT_SCALE
+    pot = ANIPotential(precision="f16x3x1", device=cuda_device, seed=0, output_scale=MD_OUTPUT_SCALE)
+    s = water_box(6, seed=5)
+    de, rmse = errors(pot, s.coordinates, s.species, [s.natoms], s.cell[None])
+    assert de <= 1e-6 and rmse <= 5e-3, (de, rmse)
+
+
+def test_f16_form_matches_fp32_form(cuda_device):
+    s = water_box(10, seed=9)
+    p32 = ANIPotential(precision="fp32", device=cuda_device, seed=0)
+    p16 = ANIPotential(precision="f16x3x2", device=cuda_device, seed=0)
+    e32, f32 = p32.energy_and_forces(s.coordinates, s.species, [s.natoms], s.cell[None])
+    e16, f16 = p16.energy_and_forces(s.coordinates, s.species, [s.natoms], s.cell[None])
+    assert abs(float(e32[0]) - float(e16[0])) * HARTREE_TO_KCALMOL / s.natoms < 2e-5
+    rmse = float(torch.sqrt(torch.mean((f32 - f16) ** 2))) * HARTREE_TO_KCALMOL
+    assert rmse < 0.03
