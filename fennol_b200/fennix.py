@@ -568,23 +568,32 @@ class PreprocessingChain:
         if batch_index is not None and not np.array_equal(np.asarray(_host(batch_index)), expected):
             raise ValueError("atoms must be grouped by system in batch order")
         out = {**inputs, "species": species, "natoms": natoms, "batch_index": expected}
-        cells = None
+        cells = recips = None
         if "cells" in inputs:
-            cells = np.asarray(_host(inputs["cells"]), dtype=np.float32)
-            if cells.ndim == 2:
-                cells = cells[None]
+            given = np.asarray(_host(inputs["cells"]))
+            if given.ndim == 2:
+                given = given[None]
+            # the reciprocal cells as the reference forms them (check_input,
+            # preprocessing.py:1780-1781): the caller's, or the inverse of the
+            # caller's cells in their own precision; float32 in the builder (:126)
+            if "reciprocal_cells" in inputs:
+                recips = np.asarray(_host(inputs["reciprocal_cells"])).reshape(-1, 3, 3)
+            else:
+                recips = np.linalg.inv(given)
+            recips = recips.astype(np.float32)
+            cells = given.astype(np.float32)
             out["cells"] = cells
-            out["reciprocal_cells"] = np.linalg.inv(cells.astype(np.float64)).astype(np.float32)
+            out["reciprocal_cells"] = recips
         minimum_image = "minimum_image" in inputs.get("flags", {})
         if self.species_order:
             sidx = AEVConfig(species_order=self.species_order).species_index(species)
         else:
             sidx = np.zeros(nat, np.int32)
         key = (species.tobytes(), natoms.tobytes(), None if cells is None else cells.tobytes(),
-               minimum_image)
+               None if recips is None else recips.tobytes(), minimum_image)
         if key != self._layout_key:
             cl = None if cells is None else list(cells)
-            self._layout = BatchLayout(sidx, natoms, cl, minimum_image, self.device)
+            self._layout = BatchLayout(sidx, natoms, cl, minimum_image, self.device, reciprocal_cells=recips)
             self._layout_key = key
         coords = torch.as_tensor(inputs["coordinates"], dtype=torch.float32)
         coords = coords.to(self.device, non_blocking=True).reshape(-1, 3).contiguous()

@@ -179,10 +179,14 @@ class BatchLayout:
     """Static description of a batch: systems, cells, species-sorted rows.
 
     ``minimum_image`` is one flag for every periodic system or one per
-    system (minimum image when true, general periodic images otherwise)."""
+    system (minimum image when true, general periodic images otherwise).
+    ``reciprocal_cells`` (optional, like the reference's input key): used as
+    given, cast to float32; otherwise each cell is inverted in the precision
+    the caller passed it in and the inverse cast to float32, as the
+    reference's ``check_input`` does (``preprocessing.py:1780-1781``)."""
 
     def __init__(self, species_idx: np.ndarray, natoms: Sequence[int], cells=None,
-                 minimum_image: bool = True, device="cuda"):
+                 minimum_image: bool = True, device="cuda", reciprocal_cells=None):
         species_idx = np.asarray(species_idx, dtype=np.int32)
         natoms = np.asarray(natoms, dtype=np.int64).reshape(-1)
         n = int(natoms.sum())
@@ -203,12 +207,17 @@ class BatchLayout:
             cl = cells if isinstance(cells, (list, tuple)) else list(np.asarray(cells).reshape(-1, 3, 3))
             if len(cl) == 1 and B > 1:
                 cl = cl * B
+            rl = None
+            if reciprocal_cells is not None:
+                rl = list(np.asarray(reciprocal_cells).reshape(-1, 3, 3))
+                if len(rl) == 1 and B > 1:
+                    rl = rl * B
             for b, c in enumerate(cl):
                 if c is None:
                     continue
-                c32 = np.asarray(c, dtype=np.float32).reshape(3, 3)
-                cell_arr[b] = c32
-                recip_arr[b] = np.linalg.inv(c32).astype(np.float32)
+                c = np.asarray(c).reshape(3, 3)
+                cell_arr[b] = c.astype(np.float32)
+                recip_arr[b] = (np.linalg.inv(c) if rl is None else rl[b]).astype(np.float32)
                 mi = minimum_image[b] if isinstance(minimum_image, (list, tuple, np.ndarray)) \
                     else minimum_image
                 mode[b] = _lib.PBC_MINIMUM_IMAGE if mi else _lib.PBC_GENERAL

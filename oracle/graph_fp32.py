@@ -62,9 +62,12 @@ def pair_list(coordinates: np.ndarray, natoms, cells: Optional[np.ndarray] = Non
     offsets = np.concatenate([[0], np.cumsum(natoms)])
     apply_pbc = cells is not None
     if apply_pbc:
-        cells = np.array(cells, dtype=np.float32).reshape(-1, 3, 3)
         if reciprocal_cells is None:
-            reciprocal_cells = np.linalg.inv(cells)
+            # the reference inverts the caller's cells in their own precision
+            # (check_input, preprocessing.py:1780-1781) and casts the result to
+            # float32 in the builder (:126)
+            reciprocal_cells = np.linalg.inv(np.asarray(cells).reshape(-1, 3, 3))
+        cells = np.array(cells, dtype=np.float32).reshape(-1, 3, 3)
         recips = np.array(reciprocal_cells, dtype=np.float32).reshape(-1, 3, 3)
     rc2 = cutoff ** 2
     out_p1, out_p2, out_s, out_d = [], [], [], []

@@ -170,3 +170,64 @@ def test_skin_filter_matches_direct_list(pot, cuda_device):
     keep = d12 < 5.2 ** 2
     ref = {"p1": skin["p1"][keep], "p2": skin["p2"][keep], "shift": skin["shift"][keep]}
     assert sym and _same(canon, ref)
+
+
+# ---- fixtures made by the reference's own host graph builders ------------------------
+
+REF_CASES = sorted(p.stem[len("ref_"):] for p in GOLDEN.glob("ref_*.npz"))
+
+
+def _directed(nj, ns, nn):
+    """Directed edges (i, j, shift) of ELL rows, sorted."""
+    rows = np.repeat(np.arange(nn.shape[0]), nn)
+    cols = np.concatenate([np.arange(k) for k in nn]) if nn.size else np.zeros(0, int)
+    j = nj[rows, cols].astype(np.int64)
+    s = unpack_shifts(ns[rows, cols]).astype(np.int64)
+    o = np.lexsort((s[:, 2], s[:, 1], s[:, 0], j, rows))
+    return rows[o], j[o], s[o]
+
+
+@pytest.mark.parametrize("name", REF_CASES)
+def test_rows_equal_reference_builder(pot, name):
+    """Radial pair set, the skin list (if any), the directed angular
+    sub-graph and the number of triplets per centre, against FeNNol's own
+    GraphGenerator / GraphFilter / GraphAngularExtension (bit-exact)."""
+    d = dict(np.load(GOLDEN / f"ref_{name}.npz"))
+    cells = d.get("cells")
+    nat = [int(v) for v in d["natoms"]]
+    mi = bool(d["minimum_image"])
+    canon, sym, *_ = _gpu_pairs(pot, d["coordinates"], d["species"], nat, cells, 5.2, mi)
+    ref = {"p1": d["p1"], "p2": d["p2"], "shift": d["shift"].astype(np.int64)}
+    assert sym and _same(canon, ref), name
+    if "skin_p1" in d:
+        canon, sym, *_ = _gpu_pairs(pot, d["coordinates"], d["species"], nat, cells, 5.2 + float(d["skin"]), mi)
+        ref = {"p1": d["skin_p1"], "p2": d["skin_p2"], "shift": d["skin_shift"].astype(np.int64)}
+        assert sym and _same(canon, ref), name
+    *_, nj, ns, nn = _gpu_pairs(pot, d["coordinates"], d["species"], nat, cells, 3.5, mi)
+    src, dst, sh = _directed(nj, ns, nn)
+    assert np.array_equal(src, d["a_src"]) and np.array_equal(dst, d["a_dst"])
+    assert np.array_equal(sh, d["a_shift"].astype(np.int64))
+    # the AEV kernels form every unordered pair of a centre's angular neighbours
+    assert np.array_equal(nn.astype(np.int64) * (nn - 1) // 2, d["t_count"])
+
+
+@pytest.mark.parametrize("name", ["water64_mi", "molecules6", "water8_general", "two_boxes_mi"])
+def test_aev_on_reference_graphs(cuda_device, name):
+    """AEV rows of the CUDA kernels on the fixture geometries against the
+    FP64 oracle, whose pairs and triplets equal the reference builder's
+    (tests/test_ref_golden.py): a missing or extra triplet would move a row
+    far beyond the float32 tolerance."""
+    from fennol_b200.params import MLPConfig
+    from oracle import ani_ref
+
+    d = dict(np.load(GOLDEN / f"ref_{name}.npz"))
+    cells = d.get("cells")
+    nat = [int(v) for v in d["natoms"]]
+    mi = bool(d["minimum_image"])
+    p = ANIPotential(precision="fp32", device=cuda_device, minimum_image=mi)
+    p.energy_and_forces(d["coordinates"], d["species"], nat, cells)
+    layout, g, ws = next(iter(p._cache.values()))
+    got = ws.x.float().cpu().numpy()[layout.atom_row_host, :1008]
+    r = ani_ref.energy_and_forces(d["coordinates"], d["species"], nat, p.weights, AEVConfig(), MLPConfig(),
+                                  cells=cells, minimum_image=mi, need_forces=False, return_aev=True)
+    np.testing.assert_allclose(got, r["aev"], rtol=1e-4, atol=2e-5)
