@@ -1,24 +1,29 @@
 """Benchmark of the ANI-2x energy+force MD step on B200.
 
-The JSON line also carries: per-kernel rooflines (``kernels``), the FP32
-form on the same workload, accuracy against the FP64 oracle, the end-to-end
-public-API call with host buffers (``e2e``), the CPU oracle on the host
-cores (``cpu_baseline``), a Poisson request stream through the serving loop
-(``serving``), the training-loss gradient of a 256-molecule batch
-(``training_256mol``), the 98,304-atom 8-model ensemble against its FP32 form
-(``ensemble_98k``) and, with ``--nve-drift-steps``, the NVE energy drift.
+Default workload (the configuration the metric is quoted on): the
+98,304-atom water box (32,768 H2O, 99.4 A cube) with an 8-model ensemble,
+NVE at dt 0.5 fs, species MLPs in the fused tcgen05 FP16 split form
+(``f16x3x1``) on float32 weights (seeded N(0, 1/fan_in), not rounded), AEV in
+float32, energy sum and integrator in float64.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload water12k|water98k] [--precision bf16x3|bf16x2|bf16|fp32]
+                    [--workload water98k|water12k] [--precision f16x3x1|f16x3x2|bf16x2|fp32]
 
-A step is one MD step of the workload: BAOAB integrator (float64) ->
-neighbour list (skin filter every step, cell-list rebuild when an atom moved
-more than half the skin) -> AEV -> species MLPs -> energy -> force adjoint,
-replayed from a CUDA graph.  Inputs live in HBM; every timed step is
-bracketed by CUDA events on the launching stream and preceded by an L2 flush
-(a 512 MB write) outside the events.  Multi-GPU runs (torchrun) are
-independent replicas (weak scaling); the time is the max over ranks.
-Prints one JSON line on rank 0.
+A step is one MD step of the workload: float64 integrator -> neighbour list
+(FeNNol's rebuild stride with every step's displacement checked on the
+device) -> AEV -> species MLPs -> energy -> force adjoint, replayed from a
+CUDA graph.  Inputs live in HBM; every timed step is bracketed by CUDA events
+on the launching stream and preceded by an L2 flush (a 512 MB write) outside
+the events.  Multi-GPU runs (torchrun) are independent replicas (weak
+scaling); the time is the max over ranks.  Prints one JSON line on rank 0.
+
+Besides the headline the line carries: ``e2e`` (the FeNNol-API call
+``FENNIX.energy_and_forces`` with pinned host buffers in and out), the FP32
+form of the same workload, the other MLP forms, accuracy against the FP64
+oracle (12,288-atom box, and its 2x2x2 tiling for the 98,304-atom size),
+per-kernel rooflines, the 12,288-atom box as a secondary line, the request
+stream through the serving loop, the training-loss gradient, the NVE drift
+(``--nve-drift-steps``) and the CPU port on the host cores (``cpu_baseline``).
 """
 
 from __future__ import annotations
@@ -30,6 +35,7 @@ import subprocess
 import sys
 import threading
 import time
+from collections import OrderedDict
 
 import numpy as np
 
@@ -39,19 +45,28 @@ sys.path.insert(0, ROOT)
 METRIC = "E+F atom-steps/s (1 B200, BF16 vs FP32 form) at stated force RMSE; p50/p99 latency"
 HARTREE_TO_KCALMOL = 627.5096080305927
 MLP_FLOP_PER_ATOM = 2 * (1008 * 256 + 256 * 192 + 192 * 160 + 160 * 1) * 2  # fwd + input grad
+DEFAULT_PRECISION = "f16x3x1"
+SMS = 148
 
 WORKLOADS = {
-    "water12k": dict(n_side=16, n_models=1, thermostat="LGV", desc=(
-        "water box 12,288 atoms (4096 H2O, 49.7 A cube), Langevin 300 K gamma 1/ps, dt 0.5 fs, "
-        "skin 1.0 A, list rebuilt every nblist_stride steps (FeNNol's rule gives 40 at 0.5 fs) with "
-        "every step checked on the device (an atom moved > skin/2 since the rebuild: roll back and "
-        "shorten the stride; the value used is in neighbour_list), "
-        "ANI-2x 7-species random-init model "
-        "(MD: last layer x0.02)")),
     "water98k": dict(n_side=32, n_models=8, thermostat="NVE", desc=(
-        "water box 98,304 atoms (32768 H2O, 99.4 A cube), NVE dt 0.5 fs, skin 1.0 A (checked stride), "
-        "8-model ANI-2x ensemble (random-init, MD: last layer x0.02)")),
+        "water box 98,304 atoms (32768 H2O, 99.4 A cube), 8-model ANI-2x ensemble (independent seeds, "
+        "seeded N(0, 1/fan_in) float32 weights; MD: last layer x0.02), NVE dt 0.5 fs, skin 1.0 A, "
+        "list rebuilt every nblist_stride steps with every step's displacement checked on the device")),
+    "water12k": dict(n_side=16, n_models=1, thermostat="LGV", desc=(
+        "water box 12,288 atoms (4096 H2O, 49.7 A cube), one ANI-2x model (seeded N(0, 1/fan_in) "
+        "float32 weights; MD: last layer x0.02), Langevin 300 K gamma 1/ps, dt 0.5 fs, skin 1.0 A, "
+        "checked rebuild stride")),
 }
+
+MLP_FORMS = {"fp32": "float32 CUDA cores",
+             "bf16": "tcgen05 BF16, FP32 accumulate",
+             "bf16x2": "tcgen05 BF16 hi+lo activations, BF16 weights (2 MMAs per product)",
+             "bf16x3": "tcgen05 BF16 hi+lo activations and weights (3 MMAs, unfused)",
+             "f16x3x1": ("tcgen05 FP16 hi+lo activations and power-of-two-scaled float32 weights: "
+                         "3 MMAs forward, 1 MMA input gradient, FP32 accumulate"),
+             "f16x3x2": ("tcgen05 FP16 hi+lo activations and power-of-two-scaled float32 weights: "
+                         "3 MMAs forward, 2 MMAs input gradient, FP32 accumulate")}
 
 
 def dist_env():
@@ -124,18 +139,27 @@ def measured_peaks():
         return 6650.0, 1590.0, 1400.0, "fallback"
 
 
-def make_engine(workload, precision, device, seed=0, bf16_weights=True, output_scale=None):
+def md_weights(workload, output_scale=None, bf16_weights=False):
+    from fennol_b200.params import MD_OUTPUT_SCALE, AEVConfig, MLPConfig, init_weights
+    from fennol_b200.potential import round_weights_bf16
+
+    w = WORKLOADS[workload]
+    W = init_weights(AEVConfig(), MLPConfig(), seed=0, n_models=w["n_models"],
+                     output_scale=MD_OUTPUT_SCALE if output_scale is None else output_scale)
+    return round_weights_bf16(W) if bf16_weights else W
+
+
+def make_engine(workload, precision, device, seed=0, bf16_weights=False, output_scale=None):
+    """MD engine of a workload.  ``bf16_weights`` rounds the model to BF16
+    (the BF16-model form, reported separately)."""
     from fennol_b200.md import MDEngine
     from fennol_b200.potential import ANIPotential
     from fennol_b200.systems import water_box
 
-    from fennol_b200.params import MD_OUTPUT_SCALE
-
     w = WORKLOADS[workload]
     box = water_box(w["n_side"], seed=seed)
-    pot = ANIPotential(precision=precision, device=device, seed=0, n_models=w["n_models"],
-                       output_scale=MD_OUTPUT_SCALE if output_scale is None else output_scale,
-                       bf16_weights=bf16_weights)
+    pot = ANIPotential(precision=precision, device=device,
+                       weights=md_weights(workload, output_scale, bf16_weights))
     eng = MDEngine(pot, box.coordinates, box.species, box.cell, dt_fs=0.5, thermostat=w["thermostat"],
                    temperature=300.0, gamma_ps=1.0, skin=1.0, trigger="stride", seed=seed)
     return box, pot, eng
@@ -183,22 +207,13 @@ def time_mlp(pot, eng, reps):
 
     lay, ws = eng.layout, eng.ws
     st = torch.cuda.current_stream().cuda_stream
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
     def launch():
         call("fennol_mlp_energy_grad", pot.precision, lay.rows, lay.ntiles, lay.t_tile_species.data_ptr(),
              lay.t_tile_row.data_ptr(), C_ptr(pot.mlp.struct), ws.x.data_ptr(), _ptr(ws.x_lo),
              ws.e_rows.data_ptr(), ws.dx.data_ptr(), ws.mlp_ws.data_ptr(), ws.mlp_ws.numel(), st)
 
-    for _ in range(3):
-        launch()
-    torch.cuda.synchronize()
-    ev0.record()
-    for _ in range(reps):
-        launch()
-    ev1.record()
-    torch.cuda.synchronize()
-    return ev0.elapsed_time(ev1) / reps
+    return time_launch(launch, reps)
 
 
 def time_launch(fn, reps):
@@ -219,7 +234,8 @@ def time_launch(fn, reps):
 
 def kernel_times(pot, eng, reps=20):
     """Device time per launch (ms) of the three large kernels of a step, on
-    the current MD state: AEV forward, species MLP, AEV adjoint."""
+    the current MD state: AEV forward, species MLP, AEV adjoint; and the mean
+    radial and angular neighbour counts."""
     import torch
     from fennol_b200._lib import call
     from fennol_b200.potential import C_ptr, _ptr
@@ -246,7 +262,6 @@ def kernel_times(pot, eng, reps=20):
     ws.forces4.zero_()
     eng._initial_forces_from_current()
     mean_nbr = float(g.rad_n[:lay.n].float().mean())
-    # angular neighbours (within the angular cutoff) of the current positions, periodic cube
     from scipy.spatial import cKDTree
     box_len = float(np.asarray(eng.cell).reshape(-1, 3, 3)[0, 0, 0])
     xyz = np.mod(eng.x.cpu().numpy(), box_len)
@@ -255,9 +270,10 @@ def kernel_times(pot, eng, reps=20):
     return out, mean_nbr, mean_ang
 
 
-def profile_traffic(kernel: str, workload: str):
-    """DRAM bytes per launch of ``kernel`` on ``workload`` recorded by an ncu
-    capture in profiles/ (a line ``traffic_bytes_per_launch <kernel> <workload> <bytes>``)."""
+def profile_value(key: str, kernel: str, workload: str):
+    """A per-launch figure recorded from an ncu capture in profiles/: a line
+    ``<key> <kernel> <workload> <value>`` (keys ``traffic_bytes_per_launch``,
+    ``inst_per_launch``)."""
     d = os.path.join(ROOT, "profiles")
     try:
         names = sorted(os.listdir(d))
@@ -268,62 +284,181 @@ def profile_traffic(kernel: str, workload: str):
             with open(os.path.join(d, name)) as f:
                 for line in f:
                     parts = line.strip().strip("`").split()
-                    if len(parts) == 4 and parts[0] == "traffic_bytes_per_launch" and \
-                            parts[1] == kernel and parts[2] == workload:
+                    if len(parts) == 4 and parts[0] == key and parts[1] == kernel and parts[2] == workload:
                         return float(parts[3])
         except OSError:
             continue
     return None
 
 
-def accuracy(pot, box):
-    """Single-point error of this precision vs the FP64 oracle."""
+def present_aev_columns(species, cfg) -> int:
+    """Columns of the AEV that a system with these species can make non-zero:
+    the radial blocks of its species and the angular blocks of its species
+    pairs (the adjoint reads only those)."""
+    present = sorted(set(cfg.species_index(np.asarray(species)).tolist()))
+    s = len(present)
+    return s * cfg.radial_dist_divisions + s * (s + 1) // 2 * cfg.angular_sublength
+
+
+def rooflines(pot, eng, box, workload, precision, sm_mhz):
+    """Per-kernel rooflines of the step's three large kernels.  The MLP is
+    bound by the tensor pipe (algorithmic FLOPs against the sustained bf16
+    GEMM peak); the AEV kernels by instruction issue (warp instructions per
+    launch from an ncu capture against 148 SMs x 4 schedulers x the sampled
+    SM clock), with their HBM fraction over the algorithmic bytes beside it."""
+    hbm, tf_burst, tf_sust, src = measured_peaks()
+    kt, mean_nbr, mean_ang = kernel_times(pot, eng)
+    w = WORKLOADS[workload]
+    n = box.natoms
+    flops = MLP_FLOP_PER_ATOM * n * w["n_models"]
+    cols = present_aev_columns(box.species, pot.aev_cfg)
+    # algorithmic bytes per atom: adjoint = the present dE/dAEV columns (float32)
+    # + the row's neighbour indices + position in + force out; forward = indices
+    # + position in, the present AEV columns out (two 16-bit parts, or float32)
+    bwd_bytes = n * (cols * 4 + mean_nbr * 4 + 16 + 16)
+    aev_out = 2 if precision == "bf16" else 4
+    fwd_bytes = n * (mean_nbr * 4 + 16 + cols * aev_out)
+    clock_hz = (sm_mhz or 1965.0) * 1e6
+    kernels = {
+        "mlp": {"kernel": "k_mlp_fused", "ms_per_launch": kt["mlp"], "bound": "tensor",
+                "algorithmic_flop_per_launch": flops, "achieved": flops / (kt["mlp"] * 1e-3) / 1e12,
+                "unit": "TFLOP/s", "peak": tf_sust, "peak_source": f"{src} bf16 sustained"},
+    }
+    for name, kname, b in (("aev_backward", "k_aev_backward", bwd_bytes), ("aev_forward", "k_aev_forward", fwd_bytes)):
+        ms = kt[name]
+        inst = profile_value("inst_per_launch", kname, workload)
+        k = {"kernel": kname, "ms_per_launch": ms, "bound": "issue",
+             "algorithmic_bytes_per_launch": b, "hbm_achieved_gbs": b / (ms * 1e-3) / 1e9,
+             "hbm_frac": b / (ms * 1e-3) / 1e9 / hbm, "hbm_peak": hbm,
+             "warp_inst_per_launch": inst}
+        if inst is not None:
+            k.update(achieved=inst / (ms * 1e-3) / 1e9, unit="Gwarp-inst/s",
+                     peak=SMS * 4 * clock_hz / 1e9,
+                     peak_source=f"{SMS} SMs x 4 issue/clk x {clock_hz / 1e6:.0f} MHz (sampled)")
+        else:
+            k.update(achieved=k["hbm_achieved_gbs"], unit="GB/s", peak=hbm, peak_source=f"{src} HBM copy")
+        kernels[name] = k
+    for k in kernels.values():
+        k["frac"] = k["achieved"] / k["peak"]
+    kernels["mean_radial_neighbors"] = mean_nbr
+    kernels["mean_angular_neighbors"] = mean_ang
+    kernels["aev_columns_present"] = cols
+    return kernels
+
+
+def supercell(box, k):
+    L = box.cell[0, 0]
+    shifts = np.array([[a, b, c] for a in range(k) for b in range(k) for c in range(k)], dtype=np.float64) * L
+    xyz = (box.coordinates[None, :, :] + shifts[:, None, :]).reshape(-1, 3)
+    return xyz, np.tile(box.species, k ** 3), box.cell * k
+
+
+def accuracy(device, precision, n_models):
+    """Error of the form against the FP64 oracle for the spec's model (seeded
+    N(0, 1/fan_in) float32 weights, unscaled, not rounded): on the 12,288-atom
+    box directly, and on its 2x2x2 tiling (98,304 atoms), whose exact energy
+    is 8x the box's and whose every copy carries the box's forces."""
+    import torch
+    from fennol_b200.params import AEVConfig, MLPConfig, init_weights
+    from fennol_b200.potential import ANIPotential
+    from fennol_b200.systems import water_box
     from oracle import ani_ref
 
+    torch.set_num_threads(os.cpu_count() or 1)
+    cfg, mcfg = AEVConfig(), MLPConfig()
+    W = init_weights(cfg, mcfg, seed=0, n_models=n_models)
+    box = water_box(16, seed=0)
+    t = time.perf_counter()
+    ref = ani_ref.energy_and_forces(box.coordinates, box.species, [box.natoms], W, cfg, mcfg,
+                                    cells=box.cell[None])
+    t_oracle = time.perf_counter() - t
+    pot = ANIPotential(cfg, mcfg, weights=W, precision=precision, device=device)
+    out = {"model": f"{n_models}-model ensemble, seeded N(0, 1/fan_in) float32 weights (not rounded, "
+                    "not scaled)", "oracle": "FP64 torch-CPU restatement, autograd forces",
+           "force_rmse_tol_kcalmol_A": 0.05, "energy_tol_kcalmol_atom": 1e-4,
+           "oracle_seconds": t_oracle}
     e, f = pot.energy_and_forces(box.coordinates, box.species, [box.natoms], box.cell[None])
-    ref = ani_ref.energy_and_forces(box.coordinates, box.species, [box.natoms], pot.weights,
-                                    pot.aev_cfg, pot.mlp_cfg, cells=box.cell[None])
-    de = abs(float(e[0]) - ref["energy"][0]) * HARTREE_TO_KCALMOL / box.natoms
-    rmse = float(np.sqrt(np.mean((f.cpu().numpy() - ref["forces"]) ** 2)) * HARTREE_TO_KCALMOL)
-    return {"force_rmse_kcalmol_A": rmse, "energy_err_kcalmol_atom": de,
-            "force_rmse_tol": 0.05, "energy_tol": 1e-4}
+    out["box_12288"] = {
+        "energy_err_kcalmol_atom": abs(float(e[0]) - ref["energy"][0]) * HARTREE_TO_KCALMOL / box.natoms,
+        "force_rmse_kcalmol_A": float(np.sqrt(np.mean((f.cpu().numpy() - ref["forces"]) ** 2))
+                                      * HARTREE_TO_KCALMOL)}
+    xyz, sp, cell = supercell(box, 2)
+    e, f = pot.energy_and_forces(xyz, sp, [xyz.shape[0]], cell[None])
+    fr = np.tile(ref["forces"], (8, 1))
+    out["tiled_98304"] = {
+        "energy_err_kcalmol_atom": abs(float(e[0]) - 8 * ref["energy"][0]) * HARTREE_TO_KCALMOL / xyz.shape[0],
+        "force_rmse_kcalmol_A": float(np.sqrt(np.mean((f.cpu().numpy() - fr) ** 2)) * HARTREE_TO_KCALMOL),
+        "note": "2x2x2 tiling of the 12,288-atom box: exact reference = 8 x its energy, tiled forces"}
+    out["within_budget"] = all(v["energy_err_kcalmol_atom"] <= 1e-4 and v["force_rmse_kcalmol_A"] <= 0.05
+                               for v in (out["box_12288"], out["tiled_98304"]))
+    return out
 
 
-def e2e(pot, box, steps, warmup):
-    """Public API call per step with pinned host coordinates in and host
-    forces/energy out (single point: the neighbour list is rebuilt each call)."""
+def ani2x_fennix(precision, n_models, device, output_scale):
+    """A FeNNol model description of the ANI-2x network (the ``ANI_AEV`` and
+    ``SPECIES_INDEX_NET`` modules with FeNNol's graph preprocessing) built
+    through the FeNNol-compatible API, with the workload's ensemble."""
+    from fennol_b200.fennix import FENNIX
+    from fennol_b200.params import ANI2X_SPECIES, AEVConfig, MLPConfig, init_weights, weights_to_variables
+
+    sp = list(ANI2X_SPECIES)
+    modules = OrderedDict(
+        embedding=dict(module_name="ANI_AEV", species_order=sp, graph_angle_key="graph_angle", radial_eta=19.7,
+                       angular_eta=12.5, radial_dist_divisions=16, angular_dist_divisions=8, zeta=14.1,
+                       angle_sections=4, radial_start=0.9, angular_start=0.9),
+        energy=dict(module_name="SPECIES_INDEX_NET", species_order=sp, activation="partial(celu,alpha=0.1)",
+                    output_dim=1, hidden_neurons=[256, 192, 160], input_key="embedding", squeeze=True))
+    prep = OrderedDict(
+        graph_filter_angle=dict(module_name="GRAPH_FILTER", cutoff=3.5, graph_key="graph_angle",
+                                parent_graph="graph"),
+        angle_extension=dict(module_name="GRAPH_ANGULAR_EXTENSION", graph_key="graph_angle"),
+        species_indexer=dict(output_key="species_index"))
+    W = init_weights(AEVConfig(), MLPConfig(), seed=0, n_models=n_models, output_scale=output_scale)
+    return FENNIX(5.2, modules, prep, energy_terms=["energy"], precision=precision, device=device,
+                  variables=weights_to_variables(W, "energy"))
+
+
+def e2e(precision, box, n_models, device, steps, warmup):
+    """FeNNol-API single point per step: ``FENNIX.energy_and_forces`` with
+    pinned host coordinates in and host forces and energy out (the neighbour
+    list is built on every call, with FeNNol's capacity protocol)."""
     import torch
+    from fennol_b200.params import MD_OUTPUT_SCALE
 
+    model = ani2x_fennix(precision, n_models, device, MD_OUTPUT_SCALE)
     x_host = torch.tensor(box.coordinates, dtype=torch.float32).pin_memory()
     f_host = torch.empty((box.natoms, 3), dtype=torch.float32).pin_memory()
     e_host = torch.empty(1, dtype=torch.float64).pin_memory()
-    dev = pot.device
-    x_dev = torch.empty_like(x_host, device=dev)
-    for _ in range(warmup):
-        x_dev.copy_(x_host, non_blocking=True)
-        e, f = pot.energy_and_forces(x_dev, box.species, [box.natoms], box.cell[None])
-    torch.cuda.synchronize()
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
-    t0.record()
-    for _ in range(steps):
-        x_dev.copy_(x_host, non_blocking=True)
-        e, f = pot.energy_and_forces(x_dev, box.species, [box.natoms], box.cell[None])
+    args = dict(species=box.species, natoms=np.array([box.natoms]), cells=box.cell[None],
+                flags={"minimum_image": True})
+
+    def call():
+        e, f, _ = model.energy_and_forces(coordinates=x_host, **args)
         f_host.copy_(f, non_blocking=True)
         e_host.copy_(e[:1], non_blocking=True)
         torch.cuda.current_stream().synchronize()
+
+    for _ in range(warmup):
+        call()
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(steps):
+        call()
     t1.record()
     torch.cuda.synchronize()
     ms = t0.elapsed_time(t1) / steps
     return {"value": box.natoms / (ms * 1e-3), "unit": "atom-steps/s", "ms_per_step": ms,
             "h2d_bytes_per_step": int(x_host.numel() * 4),
             "d2h_bytes_per_step": int(f_host.numel() * 4 + 8),
-            "api": "ANIPotential.energy_and_forces (single point, list rebuilt every call)"}
+            "api": ("fennix.FENNIX.energy_and_forces (FeNNol API: preprocessing chain with capacity "
+                    "checks, list rebuilt every call), host buffers in and out")}
 
 
-def cpu_baseline(box, n_models, samples=1):
-    """The CPU oracle (float32 torch restatement of the reference formulas,
-    numpy float32 pair search) timed on this host's cores."""
+def cpu_baseline(box, n_models, samples=1, warmup=0):
+    """The CPU port of the reference algorithm (float32 torch restatement of
+    the formulas with autograd forces, numpy float32 all-pairs search) timed
+    on this host's cores, on one box per sample."""
     import torch
     from fennol_b200.params import AEVConfig, MLPConfig, init_weights
     from oracle import ani_ref
@@ -333,56 +468,47 @@ def cpu_baseline(box, n_models, samples=1):
     cfg, mcfg = AEVConfig(), MLPConfig()
     W = init_weights(cfg, mcfg, seed=0, n_models=n_models)
     ts = []
-    for _ in range(samples):
+    for k in range(warmup + samples):
         t = time.perf_counter()
         ani_ref.energy_and_forces(box.coordinates, box.species, [box.natoms], W, cfg, mcfg,
                                   cells=box.cell[None], dtype=torch.float32)
-        ts.append(time.perf_counter() - t)
-    sec = float(np.median(ts))
+        if k >= warmup:
+            ts.append(time.perf_counter() - t)
+    sec = float(np.mean(ts))
     return {"value": box.natoms / sec, "unit": "atom-steps/s", "cores": cores, "kind": "port",
-            "sample": (f"{samples} single-point E+F of the {box.natoms}-atom box "
-                       f"(pair search + AEV + {n_models}-model MLP + autodiff forces), "
-                       f"float32, {sec:.2f} s each")}
+            "seconds_per_sample": sec, "samples": samples,
+            "sample": (f"single-point E+F of the {box.natoms}-atom water box with the {n_models}-model "
+                       f"ensemble (all-pairs search + AEV + MLPs + autodiff forces), float32, "
+                       f"{sec:.2f} s each; a bounded sample of the 98,304-atom workload, whose per-atom "
+                       f"cost on the CPU is higher (the all-pairs search grows as N^2)")}
 
 
-def ensemble_98k(device, steps, warmup, flush):
-    """The 98,304-atom water box with the 8-model ensemble: BF16 tensor-core
-    form against the float32 CUDA-core form, same MD step, same timing rules."""
+def step_line(workload, precision, device, steps, warmup, flush, bf16_weights=False):
+    """Throughput of one workload in one MLP form (single GPU)."""
     import torch
 
-    w = WORKLOADS["water98k"]
-    hbm, tf_burst, tf_sust, src = measured_peaks()
-    out = {"workload": w["desc"], "atoms": 0, "models": w["n_models"]}
-    for precision in ("bf16x2", "fp32"):
-        box, pot, eng = make_engine("water98k", precision, device)
-        ms, _ = time_steps(eng, steps, warmup, flush)
-        mlp_ms = time_mlp(pot, eng, 5)
-        flops = MLP_FLOP_PER_ATOM * box.natoms * w["n_models"]
-        out["atoms"] = box.natoms
-        out[precision] = {"value": box.natoms / (float(ms.mean()) * 1e-3), "unit": "atom-steps/s",
-                          "ms_per_step": float(ms.mean()), "mlp_ms_per_launch": mlp_ms,
-                          "mlp_tflops": flops / (mlp_ms * 1e-3) / 1e12,
-                          "mlp_frac_of_peak": flops / (mlp_ms * 1e-3) / 1e12 / tf_sust,
-                          "peak": f"{src} bf16 sustained {tf_sust} TFLOP/s"}
-        del eng, pot
-        torch.cuda.empty_cache()
-    out["speedup_vs_fp32_form"] = out["bf16x2"]["value"] / out["fp32"]["value"]
-    return out
+    box, pot, eng = make_engine(workload, precision, device, bf16_weights=bf16_weights)
+    ms, _ = time_steps(eng, steps, warmup, flush)
+    res = {"value": box.natoms / (float(ms.mean()) * 1e-3), "unit": "atom-steps/s",
+           "ms_per_step": float(ms.mean()), "mlp_ms_per_launch": time_mlp(pot, eng, 5),
+           "mlp": MLP_FORMS[precision]}
+    del eng, pot
+    torch.cuda.empty_cache()
+    return res
 
 
 DRIFT_OUTPUT_SCALE = 0.002
 
 
-def nve_drift(device, steps, workload="water98k", every=100):
-    """Total-energy record of an NVE run of the workload (BF16 MLP form,
-    float64 integrator): linear drift and largest excursion per atom.
+def nve_drift(device, steps, workload="water98k", every=100, precision=DEFAULT_PRECISION):
+    """Total-energy record of an NVE run of the workload (float64
+    integrator): linear drift and largest excursion per atom.
 
     The random-weight network has no repulsive core: over thousands of steps
-    its wells gather atoms until one centre has more angular neighbours than
-    the kernels hold.  The drift run therefore scales the last layer by
+    its wells gather atoms.  The drift run therefore scales the last layer by
     ``DRIFT_OUTPUT_SCALE`` (atomic energies well below kT), and stops early,
     saying so, if a list limit is hit."""
-    box, pot, eng = make_engine(workload, "bf16x2", device, output_scale=DRIFT_OUTPUT_SCALE)
+    box, pot, eng = make_engine(workload, precision, device, output_scale=DRIFT_OUTPUT_SCALE)
     n = box.natoms
     t_ps, etot = [], []
     done = 0
@@ -404,7 +530,7 @@ def nve_drift(device, steps, workload="water98k", every=100):
     e = np.array(etot) / n
     slope = float(np.polyfit(np.array(t_ps), e, 1)[0]) if len(e) > 2 else 0.0
     return {"workload": WORKLOADS[workload]["desc"] + f"; last layer x{DRIFT_OUTPUT_SCALE} for this run",
-            "steps": done, "stopped": stopped, "dt_fs": eng.dt * 1000.0,
+            "precision": precision, "steps": done, "stopped": stopped, "dt_fs": eng.dt * 1000.0,
             "samples": len(e), "drift_kcalmol_atom_per_ns": slope * 1000.0,
             "max_abs_dev_kcalmol_atom": float(np.abs(e - e[0]).max()),
             "e0_kcalmol_atom": float(e[0]), "temperature_end_K": eng.temperature(),
@@ -442,10 +568,10 @@ def training_256(device, reps=5):
     return {"batch": "256 molecules, 10-40 atoms (random-walk chains, H50/C30/N7/O8/S2/F2/Cl1)",
             "atoms": int(nat.sum()), "ms_per_gradient": ms, "atoms_per_s": float(nat.sum()) / (ms * 1e-3),
             "loss": terms.loss, "loss_terms": "mean (E - E_teacher)^2 + 10 mean (F - F_teacher)^2",
-            "path": "CUDA E/F + AEV tangent kernel + float32 network sweep (cuBLAS GEMMs), host time per call"}
+            "path": getattr(lg, "path_description", "CUDA E/F + AEV tangent kernel + network sweep")}
 
 
-def serving_run(device, n_requests=1000, rate_hz=2000.0, seed=0):
+def serving_run(device, n_requests=1000, rate_hz=2000.0, seed=0, precision=DEFAULT_PRECISION):
     """Poisson stream through the continuous-batching loop (real time):
     throughput of the energy/force work done and p50/p99 request latency."""
     from fennol_b200.params import MD_OUTPUT_SCALE
@@ -454,8 +580,7 @@ def serving_run(device, n_requests=1000, rate_hz=2000.0, seed=0):
                                      serve_requests_from_stream)
     from fennol_b200.systems import request_stream
 
-    pot = ANIPotential(precision="bf16x2", device=device, seed=0, output_scale=MD_OUTPUT_SCALE,
-                       bf16_weights=True)
+    pot = ANIPotential(precision=precision, device=device, seed=0, output_scale=MD_OUTPUT_SCALE)
     stream = request_stream(n_requests, rate_hz=rate_hz, seed=seed, md_steps=100, pool_size=48)
     warm = serve_requests_from_stream(request_stream(24, rate_hz=rate_hz, seed=seed + 1, md_steps=10,
                                                      pool_size=8))
@@ -468,7 +593,7 @@ def serving_run(device, n_requests=1000, rate_hz=2000.0, seed=0):
     work = atom_steps(res, {q.rid: q for q in reqs})
     lat = latency_percentiles(res)
     n_md = sum(q.kind == "md" for q in reqs)
-    return {"value": work / wall, "unit": "atom-steps/s", "wall_s": wall,
+    return {"value": work / wall, "unit": "atom-steps/s", "wall_s": wall, "precision": precision,
             "requests": len(reqs), "md_requests": n_md,
             "atoms_mean": float(np.mean([q.natoms for q in reqs])),
             "latency_ms": {"p50": lat["p50_ms"], "p99": lat["p99_ms"], "mean": lat["mean_ms"]},
@@ -479,21 +604,23 @@ def serving_run(device, n_requests=1000, rate_hz=2000.0, seed=0):
 
 
 def run_reference(args):
-    """Reference arm: the CPU restatement of the reference algorithm, one
-    bounded MD-step sample per timed step, rank 0 only."""
+    """Reference arm: the CPU port of the reference algorithm on the host
+    cores, one bounded sample of the workload per step, rank 0 only."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
     from fennol_b200.systems import water_box
     w = WORKLOADS[args.workload]
-    box = water_box(w["n_side"], seed=0)
-    steps = max(1, min(args.steps, 3))
-    base = cpu_baseline(box, w["n_models"], samples=steps)
+    # the 98,304-atom box needs 4.8e9 all-pairs candidates per step on the CPU;
+    # a step of this arm is the 12,288-atom box with the workload's ensemble
+    box = water_box(min(w["n_side"], 16), seed=0)
+    base = cpu_baseline(box, w["n_models"], samples=args.steps, warmup=args.warmup)
     line = {"metric": METRIC, "value": base["value"], "unit": "atom-steps/s", "n_gpus": world,
-            "steps": steps, "warmup": 0, "ms_per_step": box.natoms / base["value"] * 1e3,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": base["seconds_per_sample"] * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": w["desc"]},
+            "config": {"workload": w["desc"], "sample": base["sample"]},
             "cpu_baseline": base,
             "e2e": {"value": base["value"], "unit": "atom-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
@@ -505,17 +632,18 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
-    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="water12k", choices=list(WORKLOADS))
-    ap.add_argument("--precision", default=None)
+    ap.add_argument("--workload", default="water98k", choices=list(WORKLOADS))
+    ap.add_argument("--precision", default=DEFAULT_PRECISION, choices=list(MLP_FORMS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--skip-98k", action="store_true", help="skip the 98k-atom 8-model comparison")
+    ap.add_argument("--quick", action="store_true",
+                    help="headline, e2e and rooflines only (no comparisons, accuracy or side runs)")
     ap.add_argument("--skip-serving", action="store_true", help="skip the request-stream run")
     ap.add_argument("--skip-training", action="store_true", help="skip the training-gradient timing")
     ap.add_argument("--nve-drift-steps", type=int, default=0,
-                    help="also record NVE energy drift of the 98k-atom ensemble over this many steps")
+                    help="also record the NVE energy drift of the 98k-atom ensemble over this many steps")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -533,18 +661,9 @@ def main():
     device = torch.device(f"cuda:{local}")
     torch.cuda.set_device(device)
 
-    from fennol_b200 import _lib
     precision = args.precision
-    if precision is None:
-        precision = "bf16x2" if os.environ.get("FENNOL_BENCH_FP32_ONLY") is None else "fp32"
     w = WORKLOADS[args.workload]
-    try:
-        box, pot, eng = make_engine(args.workload, precision, device, seed=rank)
-    except _lib.FennolError as err:
-        if err.code != _lib.ERR_UNSUPPORTED:
-            raise
-        precision = "fp32"
-        box, pot, eng = make_engine(args.workload, precision, device, seed=rank)
+    box, pot, eng = make_engine(args.workload, precision, device, seed=rank)
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
 
     if world > 1:
@@ -558,109 +677,79 @@ def main():
         total_ms = max_over_ranks(total_ms, device)
         dist.barrier()
     value = world * box.natoms * args.steps / (total_ms * 1e-3)
+    clk = clocks.summary()
 
     res = {"metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-           "dtype": "bf16" if precision.startswith("bf16") else "f32", "data": "synthetic",
-           "config": {"workload": w["desc"], "atoms_per_gpu": box.natoms, "precision": precision,
-                      "weights": "BF16-representable (seeded N(0, 1/fan_in) rounded to BF16)",
-                      "mlp_precision": {"fp32": "float32 CUDA cores",
-                                        "bf16": "tcgen05 BF16, FP32 accumulate",
-                                        "bf16x2": "tcgen05 BF16 hi+lo activations (2 MMAs)",
-                                        "bf16x3": "tcgen05 BF16 hi+lo activations and weights (3 MMAs)"}[precision],
-                      "aev": "float32", "integrator": "float64",
+           "dtype": {"fp32": "f32", "f16x3x1": "f16", "f16x3x2": "f16"}.get(precision, "bf16"),
+           "data": "synthetic",
+           "config": {"workload": w["desc"], "atoms_per_gpu": box.natoms, "models": w["n_models"],
+                      "precision": precision, "mlp_precision": MLP_FORMS[precision],
+                      "weights": ("seeded N(0, 1/fan_in) float32 weights, not rounded (MD runs scale the "
+                                  "last layer by 0.02; accuracy uses the unscaled model)"),
+                      "aev": "float32", "energy_sum_and_integrator": "float64",
                       "l2": "flushed between timed steps (512 MB write outside the events)",
                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
            "latency_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99))},
-           "clocks": clocks.summary(),
+           "clocks": clk,
            "gpu_launches": eng.launches_per_step() * args.steps + eng.rebuild_launches() * rebuilds,
            "rebuilds_in_run": rebuilds,
            "neighbour_list": {"trigger": eng.trigger, "nblist_stride": eng.nblist_stride,
                               "stride_shortenings": eng.stride_reductions}}
-    # end-to-end public-API calls on every rank; the job rate uses the slowest rank
-    e2e_res = e2e(pot, box, max(5, args.steps // 3), 3)
+    if rank == 0:
+        kernels = rooflines(pot, eng, box, args.workload, precision, clk.get("sm_mhz"))
+        res["kernels"] = kernels
+        top = max(("aev_backward", "aev_forward", "mlp"), key=lambda k: kernels[k]["ms_per_launch"])
+        kd = kernels[top]
+        res["roofline"] = {"bound": kd["bound"], "kernel": kd["kernel"], "achieved": kd["achieved"],
+                           "peak": kd["peak"], "unit": kd["unit"], "frac": kd["frac"],
+                           "traffic": profile_value("traffic_bytes_per_launch", kd["kernel"], args.workload),
+                           "peak_source": kd["peak_source"], "ms_per_launch": kd["ms_per_launch"],
+                           "algorithmic_per_launch": kd.get("algorithmic_flop_per_launch",
+                                                            kd.get("algorithmic_bytes_per_launch"))}
+    del eng, pot
+    torch.cuda.empty_cache()
+    # end-to-end FeNNol-API calls on every rank; the job rate uses the slowest rank
+    e2e_res = e2e(precision, box, w["n_models"], device, max(5, args.steps // 4), 2)
     if world > 1:
         from fennol_b200.replicas import max_over_ranks
         ms_e2e = max_over_ranks(e2e_res["ms_per_step"], device)
         e2e_res.update(value=world * box.natoms / (ms_e2e * 1e-3), ms_per_step=ms_e2e,
                        h2d_bytes_per_step=world * e2e_res["h2d_bytes_per_step"],
                        d2h_bytes_per_step=world * e2e_res["d2h_bytes_per_step"])
+    res["e2e"] = e2e_res
     # the comparisons below are single-GPU measurements, made at N = 1 only
-    extras = world == 1
-    if rank == 0:
-        hbm, tf_burst, tf_sust, src = measured_peaks()
-        kt, mean_nbr, mean_ang = kernel_times(pot, eng)
-        mlp_ms = kt["mlp"]
-        flops = MLP_FLOP_PER_ATOM * box.natoms * w["n_models"]
-        mlp_tf = flops / (mlp_ms * 1e-3) / 1e12
-        # the per-centre staging record the forward writes and the adjoint reads:
-        # 20 B per radial edge, 28 B per angular neighbour, 4 S counters (S = 7)
-        rec = 20 * mean_nbr + 28 * mean_ang + 4 * 4 * 7
-        # algorithmic bytes per atom of the adjoint: its dE/dAEV row (float32),
-        # its staging record, the neighbour indices of its row and its force out
-        bwd_bytes = box.natoms * (1008 * 4 + rec + mean_nbr * 4 + 16)
-        # forward: neighbour row and position in, AEV row out (BF16 hi + lo or
-        # float32), staging record out
-        fwd_bytes = box.natoms * (mean_nbr * 8 + 16 + 1008 * (2 if precision == "bf16" else 4) + rec)
-        kernels = {
-            "aev_backward": {"ms_per_launch": kt["aev_backward"], "bound": "hbm",
-                             "algorithmic_bytes_per_launch": bwd_bytes,
-                             "achieved": bwd_bytes / (kt["aev_backward"] * 1e-3) / 1e9, "unit": "GB/s",
-                             "peak": hbm},
-            "aev_forward": {"ms_per_launch": kt["aev_forward"], "bound": "hbm",
-                            "algorithmic_bytes_per_launch": fwd_bytes,
-                            "achieved": fwd_bytes / (kt["aev_forward"] * 1e-3) / 1e9, "unit": "GB/s",
-                            "peak": hbm},
-            "mlp": {"ms_per_launch": mlp_ms, "bound": "tensor", "algorithmic_flop_per_launch": flops,
-                    "achieved": mlp_tf, "unit": "TFLOP/s", "peak": tf_burst},
-        }
-        for k in kernels.values():
-            k["frac"] = k["achieved"] / k["peak"]
-        res["kernels"] = kernels
-        res["kernels"]["mean_radial_neighbors"] = mean_nbr
-        res["kernels"]["mean_angular_neighbors"] = mean_ang
-        top = max(("aev_backward", "aev_forward", "mlp"), key=lambda k: kernels[k]["ms_per_launch"])
-        kd = kernels[top]
-        names = {"aev_backward": "k_aev_backward", "aev_forward": "k_aev_forward", "mlp": "k_mlp_fused"}
-        traffic = profile_traffic(names[top], args.workload)
-        res["roofline"] = {"bound": kd["bound"], "kernel": names[top], "achieved": kd["achieved"],
-                           "peak": kd["peak"], "unit": kd["unit"], "frac": kd["frac"],
-                           "traffic": traffic,
-                           "peak_source": f"{src} {'HBM copy' if kd['bound'] == 'hbm' else 'bf16 burst'}",
-                           "ms_per_launch": kd["ms_per_launch"],
-                           "algorithmic_per_launch": kd.get("algorithmic_bytes_per_launch",
-                                                            kd.get("algorithmic_flop_per_launch"))}
-        if precision != "fp32" and extras:
-            _, pot32, eng32 = make_engine(args.workload, "fp32", device, seed=rank)
-            ms32, _ = time_steps(eng32, max(5, args.steps // 3), 3, flush)
-            v32 = box.natoms / (float(ms32.mean()) * 1e-3)
-            res["fp32_form"] = {"value": v32, "ms_per_step": float(ms32.mean()),
-                                "mlp_ms_per_launch": time_mlp(pot32, eng32, 10)}
-            res["speedup_vs_fp32_form"] = value / world / v32
-            del eng32, pot32
-        if extras:
-            from fennol_b200.potential import ANIPotential
-            spec = ANIPotential(precision=precision, device=device, seed=0, n_models=w["n_models"],
-                                bf16_weights=True)
-            res["accuracy_vs_fp64_oracle"] = accuracy(spec, box)
-            res["accuracy_vs_fp64_oracle"]["model"] = ("unscaled N(0, 1/fan_in) random-init weights "
-                                                       "rounded to BF16 (same weights in the oracle)")
-            del spec
-        res["e2e"] = e2e_res
-        if not args.skip_serving and extras:
+    extras = world == 1 and rank == 0 and not args.quick
+    if extras:
+        if precision != "fp32":
+            res["fp32_form"] = step_line(args.workload, "fp32", device, max(5, args.steps // 4), 3, flush)
+            res["speedup_vs_fp32_form"] = value / world / res["fp32_form"]["value"]
+        forms = {}
+        for p, rounded in (("f16x3x2", False), ("bf16x2", True)):
+            if p != precision:
+                r = step_line(args.workload, p, device, max(5, args.steps // 4), 3, flush, bf16_weights=rounded)
+                if rounded:
+                    r["weights"] = "the same model rounded to BF16 (a different model: exact only for BF16 weights)"
+                forms[p if not rounded else "bf16x2_bf16_model"] = r
+        res["other_forms"] = forms
+        res["accuracy_vs_fp64_oracle"] = accuracy(device, precision, w["n_models"])
+        if args.workload != "water12k":
+            c2 = step_line("water12k", precision, device, args.steps, 3, flush)
+            c2["fp32_form"] = step_line("water12k", "fp32", device, max(5, args.steps // 4), 3, flush)
+            c2["speedup_vs_fp32_form"] = c2["value"] / c2["fp32_form"]["value"]
+            c2["workload"] = WORKLOADS["water12k"]["desc"]
+            res["water12k"] = c2
+        if not args.skip_serving:
             res["serving"] = serving_run(device)
-        if not args.skip_training and extras:
+        if not args.skip_training:
             res["training_256mol"] = training_256(device)
-        if not args.skip_98k and args.workload != "water98k" and extras:
-            # last: the 98k-atom engines hold several GB that later parts would work around
-            del eng, pot
-            torch.cuda.empty_cache()
-            res["ensemble_98k"] = ensemble_98k(device, 5, 3, flush)
-        if args.nve_drift_steps > 0 and extras:
+        if args.nve_drift_steps > 0:
             res["nve_drift"] = nve_drift(device, args.nve_drift_steps)
-        if not args.no_cpu_baseline and extras:
-            res["cpu_baseline"] = cpu_baseline(box, w["n_models"])
+        if not args.no_cpu_baseline:
+            from fennol_b200.systems import water_box
+            res["cpu_baseline"] = cpu_baseline(water_box(min(w["n_side"], 16), seed=0), w["n_models"])
+    if rank == 0:
         print(json.dumps(res), flush=True)
     if world > 1:
         dist.barrier()
