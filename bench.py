@@ -209,9 +209,10 @@ def time_mlp(pot, eng, reps):
     st = torch.cuda.current_stream().cuda_stream
 
     def launch():
-        call("fennol_mlp_energy_grad", pot.precision, lay.rows, lay.ntiles, lay.t_tile_species.data_ptr(),
+        call("fennol_mlp_energy_grad_active", pot.precision, lay.rows, lay.ntiles, lay.t_tile_species.data_ptr(),
              lay.t_tile_row.data_ptr(), C_ptr(pot.mlp.struct), ws.x.data_ptr(), _ptr(ws.x_lo),
-             ws.e_rows.data_ptr(), ws.dx.data_ptr(), ws.mlp_ws.data_ptr(), ws.mlp_ws.numel(), st)
+             pot.active_chunks(lay.species_mask), ws.e_rows.data_ptr(), ws.dx.data_ptr(), ws.mlp_ws.data_ptr(),
+             ws.mlp_ws.numel(), st)
 
     return time_launch(launch, reps)
 

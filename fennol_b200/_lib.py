@@ -96,6 +96,8 @@ _SIGNATURES = {
     "fennol_aev_tangent": (I, [P, I, P, P, P, P, P, I, C.POINTER(AEVParams), P, P, P, I, P, P]),
     "fennol_mlp_workspace_bytes": (SZ, [I, I, I, C.POINTER(MLPWeights)]),
     "fennol_mlp_energy_grad": (I, [I, I, I, P, P, C.POINTER(MLPWeights), P, P, P, P, P, SZ, P]),
+    "fennol_mlp_energy_grad_active": (I, [I, I, I, P, P, C.POINTER(MLPWeights), P, P, ULL, P, P, P, SZ, P]),
+    "fennol_aev_active_chunks": (ULL, [C.POINTER(AEVParams), C.c_uint]),
     "fennol_energy_workspace_bytes": (SZ, [I, I]),
     "fennol_energy_reduce": (I, [P, P, I, P, I, D, P, P, P, SZ, P]),
     "fennol_forces_finalize": (I, [P, I, F, P, P]),
@@ -113,7 +115,7 @@ _lib: Optional[C.CDLL] = None
 def declared_symbols():
     """Function names declared in the public header."""
     txt = HEADER.read_text()
-    return sorted(set(re.findall(r"^\s*(?:const\s+)?[a-z_0-9]+\**\s+\**(fennol_[a-z_0-9]+)\s*\(",
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?(?:[a-z_0-9]+\s+)*[a-z_0-9]+\**\s+\**(fennol_[a-z_0-9]+)\s*\(",
                                  txt, flags=re.M)))
 
 

@@ -1026,6 +1026,27 @@ extern "C" int fennol_aev_length(const fennol_aev_params* p) {
   return k.F;
 }
 
+extern "C" unsigned long long fennol_aev_active_chunks(const fennol_aev_params* p, unsigned species_mask) {
+  if (fennol_aev_length(p) <= 0) return 0ull;
+  const int S = p->num_species, RD = p->radial_divisions;
+  const int A = p->angular_divisions * p->angle_sections;
+  const int F = S * RD + S * (S + 1) / 2 * A;
+  if (F > 64 * 64) return 0ull;
+  unsigned long long m = 0ull;
+  auto mark = [&](int c0, int c1) {  // columns [c0, c1)
+    for (int c = c0 / 64; c <= (c1 - 1) / 64; ++c) m |= 1ull << c;
+  };
+  for (int s = 0; s < S; ++s)
+    if ((species_mask >> s) & 1u) mark(s * RD, (s + 1) * RD);
+  for (int s1 = 0; s1 < S; ++s1)
+    for (int s2 = s1; s2 < S; ++s2)
+      if (((species_mask >> s1) & 1u) && ((species_mask >> s2) & 1u)) {
+        const int c0 = S * RD + fnl::triu_pair(s1, s2, S) * A;
+        mark(c0, c0 + A);
+      }
+  return m;
+}
+
 extern "C" int fennol_pack_atoms(const float* coords, const int* species_idx, int natoms, float* xyzs,
                                  void* stream) {
   if (natoms < 0 || (natoms > 0 && (!coords || !species_idx || !xyzs))) return FENNOL_ERR_INVALID;

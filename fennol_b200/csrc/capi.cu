@@ -29,10 +29,10 @@ extern "C" size_t fennol_mlp_workspace_bytes(int precision, int rows, int n_mode
   return fnl_mlp_tc_workspace(precision, rows, n_models, w);
 }
 
-extern "C" int fennol_mlp_energy_grad(int precision, int rows, int ntiles, const int* tile_species,
-                                      const int* tile_row, const fennol_mlp_weights* w, const void* x,
-                                      const void* x_lo, float* e_rows, float* dx, void* workspace,
-                                      size_t workspace_bytes, void* stream) {
+extern "C" int fennol_mlp_energy_grad_active(int precision, int rows, int ntiles, const int* tile_species,
+                                             const int* tile_row, const fennol_mlp_weights* w, const void* x,
+                                             const void* x_lo, unsigned long long active_chunks, float* e_rows,
+                                             float* dx, void* workspace, size_t workspace_bytes, void* stream) {
   if (precision < FENNOL_MLP_FP32 || precision > FENNOL_MLP_F16X3X2) return FENNOL_ERR_INVALID;
   if (!weights_ok(precision, w)) return FENNOL_ERR_INVALID;
   if (rows < 0 || ntiles < 0 || rows % 128 != 0 || ntiles * 128 > rows) return FENNOL_ERR_INVALID;
@@ -44,6 +44,15 @@ extern "C" int fennol_mlp_energy_grad(int precision, int rows, int ntiles, const
   if (precision == FENNOL_MLP_FP32)
     return fnl_mlp_simt(rows, ntiles, tile_species, tile_row, w, (const float*)x, e_rows, dx, workspace, st);
   if (precision != FENNOL_MLP_BF16 && !x_lo) return FENNOL_ERR_INVALID;
-  return fnl_mlp_tc(precision, rows, ntiles, tile_species, tile_row, w, x, x_lo, e_rows, dx, workspace,
-                    workspace_bytes, st);
+  if (!active_chunks) return FENNOL_ERR_INVALID;
+  return fnl_mlp_tc(precision, rows, ntiles, tile_species, tile_row, w, x, x_lo, active_chunks, e_rows, dx,
+                    workspace, workspace_bytes, st);
+}
+
+extern "C" int fennol_mlp_energy_grad(int precision, int rows, int ntiles, const int* tile_species,
+                                      const int* tile_row, const fennol_mlp_weights* w, const void* x,
+                                      const void* x_lo, float* e_rows, float* dx, void* workspace,
+                                      size_t workspace_bytes, void* stream) {
+  return fennol_mlp_energy_grad_active(precision, rows, ntiles, tile_species, tile_row, w, x, x_lo, ~0ull, e_rows,
+                                       dx, workspace, workspace_bytes, stream);
 }

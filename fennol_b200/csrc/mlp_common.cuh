@@ -23,10 +23,10 @@ int fnl_mlp_simt(int rows, int ntiles, const int* tile_species, const int* tile_
                  cudaStream_t st);
 size_t fnl_mlp_tc_workspace(int precision, int rows, int n_models, const fennol_mlp_weights* w);
 int fnl_mlp_tc(int precision, int rows, int ntiles, const int* tile_species, const int* tile_row,
-               const fennol_mlp_weights* w, const void* x, const void* x_lo, float* e_rows, float* dx,
-               void* ws, size_t ws_bytes, cudaStream_t st);
+               const fennol_mlp_weights* w, const void* x, const void* x_lo, unsigned long long kmask,
+               float* e_rows, float* dx, void* ws, size_t ws_bytes, cudaStream_t st);
 bool fnl_mlp_fused_supported(int precision, const fennol_mlp_weights* w);
 size_t fnl_mlp_fused_workspace(const fennol_mlp_weights* w);
 int fnl_mlp_fused(int precision, int rows, int ntiles, const int* tile_species, const int* tile_row,
-                  const fennol_mlp_weights* w, const void* x, const void* x_lo, float* e_rows, float* dx,
-                  void* ws, size_t ws_bytes, cudaStream_t st);
+                  const fennol_mlp_weights* w, const void* x, const void* x_lo, unsigned long long kmask,
+                  float* e_rows, float* dx, void* ws, size_t ws_bytes, cudaStream_t st);

@@ -25,6 +25,10 @@
 // (+ G_hi W_lo).  Each epilogue divides its accumulator by the layer's weight
 // scale; the backward chain carries the power-of-two scale of the last layer's
 // kernel until dX.
+// Active columns: bit c of kmask says that input columns [64c, 64c + 64) may
+// be non-zero (the caller guarantees the others are zero in every row).  L1
+// streams only the active K-chunks, and B1 computes dX only on runs of up to
+// four consecutive active chunks (the other dX columns are left untouched).
 // CELU' of layers 1-2 (needed by the backward) goes to a per-CTA scratch in
 // global memory that stays L2 resident.  The ensemble is processed model by
 // model inside the CTA, so the per-row energy and dE/dAEV sums are
@@ -73,6 +77,7 @@ struct FusedParams {
   int xstages;
   uint32_t xstage;
   float alpha, inv_models;
+  unsigned long long kmask;  // active 64-column chunks of the input
   const float4* scales;  // F16 forms: per group (s_W1, s_W2, s_W3, s_w4) powers of two
   const float* b1;
   const float* b2;
@@ -98,6 +103,21 @@ struct Bars {
   int abort_flag;
   float ex[BM];
 };
+
+// First active 64-column chunk at or after c and the length (at most 4) of
+// the run of consecutive active chunks that starts there; -1 when none is left.
+__device__ __forceinline__ int run_at(unsigned long long mask, int c, int& len) {
+  const unsigned long long m = c < 64 ? (mask >> c) : 0ull;
+  if (!m) {
+    len = 0;
+    return -1;
+  }
+  const int s = c + __ffsll((long long)m) - 1;
+  int l = 1;
+  while (l < 4 && s + l < 64 && ((mask >> (s + l)) & 1ull)) ++l;
+  len = l;
+  return s;
+}
 
 __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -222,7 +242,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
         for (int m = 0; m < M && ok; ++m, ++item) {
           const int g = m * p.n_species + sp;
           if (item > 0 && !(ok = wait_bar(&bars->act_free, (item - 1) & 1, abort_flag, p.err))) break;
-          for (int kc = 0; kc < p.d0 / BK; ++kc, ++xq) {
+          for (unsigned long long rest = p.kmask; rest; rest &= rest - 1, ++xq) {
+            const int kc = __ffsll((long long)rest) - 1;
             const int s = xq % XS;
             const uint32_t u = xq / XS;
             if (u > 0 && !(ok = wait_bar(&bars->x_empty[s], (u - 1) & 1, abort_flag, p.err))) break;
@@ -234,33 +255,45 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
             if (p.wf_lo) tma_load_2d(&maps.w1t_lo, &bars->x_full[s], st + 4 * kAtom, kc * BK, g * p.d1);
           }
           if (!ok) break;
-          // the weight ring lies in the last L1 stage: its last chunk of this
-          // item must have been consumed (d0 / BK >= 3, so the item used it)
+          // the weight ring lies in the last L1 stage: its latest chunk must have
+          // been consumed (a stage last used by an earlier item was, before
+          // act_free completed)
           {
             const int rs = XS - 1;
-            const uint32_t last = xq - 1 - ((xq - 1 - rs) % XS);
-            if (!(ok = wait_bar(&bars->x_empty[rs], (last / XS) & 1, abort_flag, p.err))) break;
+            if (xq > (uint32_t)rs) {
+              const uint32_t last = xq - 1 - ((xq - 1 - rs) % XS);
+              if (!(ok = wait_bar(&bars->x_empty[rs], (last / XS) & 1, abort_flag, p.err))) break;
+            }
           }
           // weight chunks of the remaining GEMMs, in MMA order
           // (a GEMM with weight low parts takes the hi and lo chunks of each K step)
-          const CUtensorMap* wm[5] = {&maps.w2t, &maps.w3t, &maps.w3, &maps.w2, &maps.w1};
-          const CUtensorMap* wml[5] = {&maps.w2t_lo, &maps.w3t_lo, &maps.w3_lo, &maps.w2_lo, &maps.w1_lo};
-          const int rows_g[5] = {p.d2, p.d3, p.d2, p.d1, p.d0};
-          const int box[5] = {p.d2, p.d3, p.d2, p.d1, 256};
-          const int nk[5] = {p.d1 / BK, p.d2 / BK, p.d3 / BK, p.d2 / BK, p.d1 / BK};
-          const int nchunk[5] = {1, 1, 1, 1, p.d0 / 256};
-          const int nt[5] = {1 + p.wf_lo, 1 + p.wf_lo, 1 + p.wb_lo, 1 + p.wb_lo, 1 + p.wb_lo};
-          for (int jb = 0; jb < 5 && ok; ++jb) {
-            for (int c = 0; c < nchunk[jb] && ok; ++c) {
-              for (int kc = 0; kc < nk[jb] && ok; ++kc) {
-                for (int t = 0; t < nt[jb]; ++t, ++wq) {
-                  const int s = wq % kWStages;
-                  const uint32_t u = wq / kWStages;
-                  if (u > 0 && !(ok = wait_bar(&bars->w_empty[s], (u - 1) & 1, abort_flag, p.err))) break;
-                  mbar_expect_tx(&bars->w_full[s], (uint32_t)box[jb] * BK * 2);
-                  tma_load_2d(t ? wml[jb] : wm[jb], &bars->w_full[s], wring + s * kWStage, kc * BK,
-                              g * rows_g[jb] + c * 256);
-                }
+          const CUtensorMap* wm[4] = {&maps.w2t, &maps.w3t, &maps.w3, &maps.w2};
+          const CUtensorMap* wml[4] = {&maps.w2t_lo, &maps.w3t_lo, &maps.w3_lo, &maps.w2_lo};
+          const int rows_g[4] = {p.d2, p.d3, p.d2, p.d1};
+          const int nk[4] = {p.d1 / BK, p.d2 / BK, p.d3 / BK, p.d2 / BK};
+          const int nt[4] = {1 + p.wf_lo, 1 + p.wf_lo, 1 + p.wb_lo, 1 + p.wb_lo};
+          for (int jb = 0; jb < 4 && ok; ++jb) {
+            for (int kc = 0; kc < nk[jb] && ok; ++kc) {
+              for (int t = 0; t < nt[jb]; ++t, ++wq) {
+                const int s = wq % kWStages;
+                const uint32_t u = wq / kWStages;
+                if (u > 0 && !(ok = wait_bar(&bars->w_empty[s], (u - 1) & 1, abort_flag, p.err))) break;
+                mbar_expect_tx(&bars->w_full[s], (uint32_t)rows_g[jb] * BK * 2);
+                tma_load_2d(t ? wml[jb] : wm[jb], &bars->w_full[s], wring + s * kWStage, kc * BK, g * rows_g[jb]);
+              }
+            }
+          }
+          // B1: W1 rows of each run of active dX chunks, 64-row boxes stacked in the stage
+          for (int len = 0, c0 = run_at(p.kmask, 0, len); c0 >= 0 && ok; c0 = run_at(p.kmask, c0 + len, len)) {
+            for (int kc = 0; kc < p.d1 / BK && ok; ++kc) {
+              for (int t = 0; t < 1 + p.wb_lo; ++t, ++wq) {
+                const int s = wq % kWStages;
+                const uint32_t u = wq / kWStages;
+                if (u > 0 && !(ok = wait_bar(&bars->w_empty[s], (u - 1) & 1, abort_flag, p.err))) break;
+                mbar_expect_tx(&bars->w_full[s], (uint32_t)len * 64 * BK * 2);
+                for (int q = 0; q < len; ++q)
+                  tma_load_2d(t ? &maps.w1_lo : &maps.w1, &bars->w_full[s], wring + s * kWStage + q * 64 * BK * 2,
+                              kc * BK, g * p.d0 + (c0 + q) * 64);
               }
             }
           }
@@ -337,7 +370,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
             if (!(ok = acquire_acc(b))) break;
             const uint32_t idesc = F16 ? idesc_f16_f32(p.d1) : idesc_bf16_f32(p.d1);
             const uint32_t d = tmem + b * 256;
-            for (int kc = 0; kc < p.d0 / BK; ++kc, ++xq) {
+            int ki = 0;
+            for (unsigned long long rest = p.kmask; rest; rest &= rest - 1, ++xq, ++ki) {
               const int s = xq % XS;
               if (!(ok = wait_bar(&bars->x_full[s], (xq / XS) & 1, abort_flag, p.err))) break;
               fence_after_sync();
@@ -346,7 +380,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
               for (int kk = 0; kk < BK / 16; ++kk) {
                 const uint64_t ad = sdesc_sw128(st + kk * 32);
                 const uint64_t bd = sdesc_sw128(st + 2 * kAtom + kk * 32);
-                mma_bf16(d, ad, bd, idesc, (kc | kk) != 0);
+                mma_bf16(d, ad, bd, idesc, (ki | kk) != 0);
                 if (p.a_lo) mma_bf16(d, sdesc_sw128(st + kAtom + kk * 32), bd, idesc, 1u);
                 if (p.wf_lo) mma_bf16(d, ad, sdesc_sw128(st + 4 * kAtom + kk * 32), idesc, 1u);
               }
@@ -370,11 +404,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
             ++job;
           }
           if (!ok) break;
-          // B1: dX chunks of 256 columns, A = G1 (published atom by atom for the first)
-          for (int c = 0; c < p.d0 / 256 && ok; ++c) {
+          // B1: dX on each run of active chunks (<= 256 columns), A = G1
+          // (published atom by atom for the first run)
+          bool first = true;
+          for (int len = 0, c0 = run_at(p.kmask, 0, len); c0 >= 0 && ok; c0 = run_at(p.kmask, c0 + len, len)) {
             const uint32_t b = job & 1;
             if (!(ok = acquire_acc(b))) break;
-            if (!(ok = gemm_act(256, p.d1, b, c == 0, p.g_lo, p.wb_lo))) break;
+            if (!(ok = gemm_act(64 * len, p.d1, b, first, p.g_lo, p.wb_lo))) break;
+            first = false;
             mma_commit(&bars->acc_full[b]);
             ++nuse[b];
             ++job;
@@ -567,10 +604,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
         uint8_t* trow = tile + lane * 128;
         const int dx_row = p.tile_row[w] + 32 * q;
         const float dx_scale = p.inv_models * (inv_s1 / s_g);
-        for (int c = 0; c < p.d0 / 256 && ok; ++c) {
+        for (int len = 0, c0 = run_at(p.kmask, 0, len); c0 >= 0 && ok; c0 = run_at(p.kmask, c0 + len, len)) {
           const uint32_t b = job & 1;
           if (!(ok = take_acc(b))) break;
-          for (int cc = half; cc < 8; cc += 2) {
+          for (int cc = half; cc < 2 * len; cc += 2) {
             float v[32];
             tmem_ld32(tmem + b * 256 + lane_base + cc * 32, v);
             if (lane == 0) bulk_wait_read();  // the tile's previous copy has read it
@@ -584,9 +621,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
             __syncwarp();
             if (lane == 0) {
               if (m == 0)
-                tma_store_2d(&maps.dx, tile, c * 256 + cc * 32, dx_row);
+                tma_store_2d(&maps.dx, tile, c0 * 64 + cc * 32, dx_row);
               else
-                tma_add_2d(&maps.dx, tile, c * 256 + cc * 32, dx_row);
+                tma_add_2d(&maps.dx, tile, c0 * 64 + cc * 32, dx_row);
               bulk_commit();
             }
           }
@@ -681,8 +718,8 @@ size_t fnl_mlp_fused_workspace(const fennol_mlp_weights* w) {
 }
 
 int fnl_mlp_fused(int precision, int rows, int ntiles, const int* tile_species, const int* tile_row,
-                  const fennol_mlp_weights* w, const void* x, const void* x_lo, float* e_rows, float* dx,
-                  void* ws, size_t ws_bytes, cudaStream_t st) {
+                  const fennol_mlp_weights* w, const void* x, const void* x_lo, unsigned long long kmask,
+                  float* e_rows, float* dx, void* ws, size_t ws_bytes, cudaStream_t st) {
   if (!encode_fn()) return FENNOL_ERR_UNSUPPORTED;
   if (ws_bytes < fnl_mlp_fused_workspace(w)) return FENNOL_ERR_WORKSPACE;
   const int* d = w->dims;
@@ -707,13 +744,13 @@ int fnl_mlp_fused(int precision, int rows, int ntiles, const int* tile_species, 
             map2d(&maps.w3t, w->wt_hi[2], (uint64_t)G * d[3], d[2], d[3], f16) &&
             map2d(&maps.w3, w->w_hi[2], (uint64_t)G * d[2], d[3], d[2], f16) &&
             map2d(&maps.w2, w->w_hi[1], (uint64_t)G * d[1], d[2], d[1], f16) &&
-            map2d(&maps.w1, w->w_hi[0], (uint64_t)G * d[0], d[1], 256, f16) &&
+            map2d(&maps.w1, w->w_hi[0], (uint64_t)G * d[0], d[1], 64, f16) &&
             map2d(&maps.w1t_lo, wtl[0], (uint64_t)G * d[1], d[0], d[1], f16) &&
             map2d(&maps.w2t_lo, wtl[1], (uint64_t)G * d[2], d[1], d[2], f16) &&
             map2d(&maps.w3t_lo, wtl[2], (uint64_t)G * d[3], d[2], d[3], f16) &&
             map2d(&maps.w3_lo, wl[2], (uint64_t)G * d[2], d[3], d[2], f16) &&
             map2d(&maps.w2_lo, wl[1], (uint64_t)G * d[1], d[2], d[1], f16) &&
-            map2d(&maps.w1_lo, wl[0], (uint64_t)G * d[0], d[1], 256, f16) && map_dx(&maps.dx, dx, rows, d[0]);
+            map2d(&maps.w1_lo, wl[0], (uint64_t)G * d[0], d[1], 64, f16) && map_dx(&maps.dx, dx, rows, d[0]);
   if (!ok) return FENNOL_ERR_CUDA;
   FusedParams p{};
   p.ntiles = ntiles;
@@ -732,6 +769,9 @@ int fnl_mlp_fused(int precision, int rows, int ntiles, const int* tile_species, 
   p.xstages = wflo ? kXStagesWide : kXStages;
   p.xstage = wflo ? kXStageWide : kXStage;
   p.scales = reinterpret_cast<const float4*>(w->f16_scale);
+  const int nck = d[0] / BK;
+  p.kmask = kmask & (nck >= 64 ? ~0ull : ((1ull << nck) - 1));
+  if (!p.kmask) return FENNOL_ERR_INVALID;
   p.alpha = w->celu_alpha;
   p.inv_models = 1.0f / (float)w->n_models;
   p.b1 = w->b32[0];

@@ -466,12 +466,13 @@ size_t fnl_mlp_tc_workspace(int precision, int rows, int n_models, const fennol_
 }
 
 int fnl_mlp_tc(int precision, int rows, int ntiles, const int* tile_species, const int* tile_row,
-               const fennol_mlp_weights* w, const void* x, const void* x_lo, float* e_rows, float* dx, void* ws,
-               size_t ws_bytes, cudaStream_t st) {
+               const fennol_mlp_weights* w, const void* x, const void* x_lo, unsigned long long kmask,
+               float* e_rows, float* dx, void* ws, size_t ws_bytes, cudaStream_t st) {
   if (!encode_fn()) return FENNOL_ERR_UNSUPPORTED;
   const bool f16 = precision == FENNOL_MLP_F16X3X1 || precision == FENNOL_MLP_F16X3X2;
   if (fnl_mlp_fused_supported(precision, w) && (f16 || !getenv("FENNOL_MLP_UNFUSED")))
-    return fnl_mlp_fused(precision, rows, ntiles, tile_species, tile_row, w, x, x_lo, e_rows, dx, ws, ws_bytes, st);
+    return fnl_mlp_fused(precision, rows, ntiles, tile_species, tile_row, w, x, x_lo, kmask, e_rows, dx, ws,
+                         ws_bytes, st);
   if (f16) return FENNOL_ERR_UNSUPPORTED;  // the FP16 forms exist only as the fused kernel
   const int* d = w->dims;
   for (int l = 0; l < 4; ++l)

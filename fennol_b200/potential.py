@@ -222,6 +222,10 @@ class BatchLayout:
                     else minimum_image
                 mode[b] = _lib.PBC_MINIMUM_IMAGE if mi else _lib.PBC_GENERAL
         self.has_pbc = bool((mode != 0).any())
+        # species present in the batch (bit s): the AEV columns of absent
+        # species and species pairs are zero in every row
+        self.species_mask = int(np.bitwise_or.reduce(1 << np.unique(np.asarray(species_idx, np.int64)))) \
+            if n else 1
         self.mode_host, self.cell_host, self.recip_host = mode, cell_arr, recip_arr
         # species-sorted rows, segments padded to the 128-row tile
         self.species_idx = species_idx
@@ -433,6 +437,7 @@ class ANIPotential:
                            "kcalpermol": HARTREE_TO_KCALMOL}[energy_unit.lower()]
         self.minimum_image = minimum_image
         self._cache: Dict[tuple, tuple] = {}
+        self._chunk_masks: Dict[int, int] = {}
         self.capacity_margin = 1.05
         self.add_neigh = 8
         # repeated calls on the same batch replay one captured CUDA graph
@@ -471,6 +476,17 @@ class ANIPotential:
         ws = Workspace(self, layout)
         return g, ws
 
+    def active_chunks(self, species_mask: int) -> int:
+        """The 64-column chunks of the AEV rows that can be non-zero for a
+        batch of these species (``fennol_aev_active_chunks``)."""
+        m = self._chunk_masks.get(species_mask)
+        if m is None:
+            m = int(_lib.load().fennol_aev_active_chunks(C_ptr(self.params), species_mask))
+            if m == 0:
+                m = (1 << 64) - 1   # widths the mask cannot describe: every column
+            self._chunk_masks[species_mask] = m
+        return m
+
     def mlp_launches(self) -> int:
         """Kernels launched by one fennol_mlp_energy_grad call: the FP32 form
         runs 7 per model, the fused tcgen05 kernel (BF16 / BF16x2 on these
@@ -506,10 +522,10 @@ class ANIPotential:
                  layout.t_cell.data_ptr(), g.rad_j.data_ptr(), g.rad_s.data_ptr(), g.rad_n.data_ptr(),
                  g.cap_r, lib_p, layout.t_atom_row.data_ptr(), ws.aev_kind, ws.x.data_ptr(),
                  _ptr(ws.x_lo), ws.x.shape[1], ws.status.data_ptr(), stream)
-        call("fennol_mlp_energy_grad", self.precision, layout.rows, layout.ntiles,
+        call("fennol_mlp_energy_grad_active", self.precision, layout.rows, layout.ntiles,
              layout.t_tile_species.data_ptr(), layout.t_tile_row.data_ptr(), C_ptr(self.mlp.struct),
-             ws.x.data_ptr(), _ptr(ws.x_lo), ws.e_rows.data_ptr(), ws.dx.data_ptr(),
-             ws.mlp_ws.data_ptr(), ws.mlp_ws.numel(), stream)
+             ws.x.data_ptr(), _ptr(ws.x_lo), self.active_chunks(layout.species_mask), ws.e_rows.data_ptr(),
+             ws.dx.data_ptr(), ws.mlp_ws.data_ptr(), ws.mlp_ws.numel(), stream)
         if ghost_rows is not None and ghost_rows.numel() > 0:
             ws.e_rows.index_fill_(0, ghost_rows, 0.0)
             ws.dx.index_fill_(0, ghost_rows, 0.0)

@@ -173,6 +173,16 @@ typedef struct fennol_aev_params {
 int fennol_aev_length(const fennol_aev_params* p);
 
 /*
+ * Host only.  The 64-column chunks of an AEV row (layout of
+ * fennol_aev_forward) that can be non-zero when the atoms' species indices
+ * all lie in species_mask (bit s = species s present): the radial blocks of
+ * the present species and the angular blocks of their pairs.  Bit c of the
+ * result covers columns [64c, 64c + 64); widths beyond 64 chunks are not
+ * representable (0 is returned, as for unsupported parameters).
+ */
+unsigned long long fennol_aev_active_chunks(const fennol_aev_params* p, unsigned species_mask);
+
+/*
  * Pack positions and species for the AEV kernels: xyzs[i] = (x, y, z,
  * species index as int bits).  species_idx are positions in species_order.
  */
@@ -339,6 +349,25 @@ int fennol_mlp_energy_grad(int precision, int rows, int ntiles, const int* tile_
                            const int* tile_row, const fennol_mlp_weights* w, const void* x,
                            const void* x_lo, float* e_rows, float* dx, void* workspace,
                            size_t workspace_bytes, void* stream);
+
+/*
+ * fennol_mlp_energy_grad for inputs whose columns are zero outside known
+ * 64-column chunks.  No separate counterpart in the reference: SpeciesIndexNet
+ * (nets.py:397-417) multiplies every column, and the ANIAEV columns of
+ * species (pairs) absent from a batch are zero there too.  Bit c of
+ * active_chunks says that columns [64c, 64c + 64) of x may be non-zero; the
+ * caller guarantees that every other column is zero in every row (for AEV
+ * rows, fennol_aev_active_chunks gives the mask of a species set).  The
+ * fused tensor-core forms then skip the inactive K-chunks of the first layer
+ * and write dx only in the active chunks (the other dx columns are left as
+ * they were: the AEV adjoint reads only blocks of species present around
+ * each centre); the other forms compute every column.  active_chunks == 0
+ * is FENNOL_ERR_INVALID; ~0 is fennol_mlp_energy_grad.
+ */
+int fennol_mlp_energy_grad_active(int precision, int rows, int ntiles, const int* tile_species,
+                                  const int* tile_row, const fennol_mlp_weights* w, const void* x,
+                                  const void* x_lo, unsigned long long active_chunks, float* e_rows,
+                                  float* dx, void* workspace, size_t workspace_bytes, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Reductions and outputs                                                    */

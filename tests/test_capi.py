@@ -124,3 +124,30 @@ def test_serving_host_helpers():
     assert abs(lat["p50_ms"] - 3.5) < 1e-9
     want = sum(q.natoms * (1 + (q.md_steps if q.kind == "md" else 0)) for q in reqs)
     assert atom_steps(res, {q.rid: q for q in reqs}) == want
+
+
+def test_aev_active_chunks_cover_every_nonzero_column():
+    """For batches with a subset of the species, every non-zero column of the
+    oracle's AEV rows lies in a chunk that fennol_aev_active_chunks reports,
+    and the mask grows with the species set."""
+    from fennol_b200.params import AEVConfig, MLPConfig, init_weights
+    from fennol_b200.potential import C_ptr, aev_params
+    from fennol_b200.systems import molecule_batch, water_box
+    from oracle import ani_ref
+
+    lib = _lib.load()
+    cfg = AEVConfig()
+    p = aev_params(cfg)
+    W = init_weights(cfg, MLPConfig(), seed=0)
+    cases = [water_box(3, seed=1)] + molecule_batch(6, seed=12)
+    for s in cases:
+        cells = None if getattr(s, "cell", None) is None else s.cell[None]
+        r = ani_ref.energy_and_forces(s.coordinates, s.species, [s.natoms], W, cfg, MLPConfig(), cells=cells,
+                                      need_forces=False, return_aev=True)
+        sidx = cfg.species_index(s.species)
+        mask = int(np.bitwise_or.reduce(1 << np.unique(sidx)))
+        chunks = lib.fennol_aev_active_chunks(C_ptr(p), mask)
+        nz = np.nonzero(np.abs(r["aev"]).max(axis=0) > 0)[0]
+        assert all((chunks >> (c // 64)) & 1 for c in nz), (mask, bin(chunks))
+        assert chunks & ~lib.fennol_aev_active_chunks(C_ptr(p), 0x7F) == 0
+    assert lib.fennol_aev_active_chunks(C_ptr(p), 0x7F) == (1 << 16) - 1

@@ -162,3 +162,42 @@ def test_f16_form_matches_fp32_form(cuda_device):
     assert abs(float(e32[0]) - float(e16[0])) * HARTREE_TO_KCALMOL / s.natoms < 2e-5
     rmse = float(torch.sqrt(torch.mean((f32 - f16) ** 2))) * HARTREE_TO_KCALMOL
     assert rmse < 0.03
+
+
+@pytest.mark.parametrize("precision", ["bf16x2", "f16x3x1", "f16x3x2"])
+def test_active_chunks_match_dense(cuda_device, precision):
+    """fennol_mlp_energy_grad_active (water: 6 of 16 input chunks active)
+    gives the dense call's row energies and its dE/dAEV on the active
+    columns; the skipped input columns are zero, so only FP32 rounding of the
+    accumulation may differ."""
+    from fennol_b200._lib import call
+    from fennol_b200.potential import C_ptr, _ptr
+
+    pot = ANIPotential(precision=precision, device=cuda_device, seed=0, n_models=2,
+                       bf16_weights=precision == "bf16x2")
+    s = water_box(6, seed=2)
+    pot.energy_and_forces(s.coordinates, s.species, [s.natoms], s.cell[None])
+    layout, g, ws = next(iter(pot._cache.values()))
+    mask = pot.active_chunks(layout.species_mask)
+    assert mask == 0b110000001111
+    st = torch.cuda.current_stream().cuda_stream
+    outs = {}
+    for name, m in (("active", mask), ("dense", None)):
+        e_rows = torch.zeros_like(ws.e_rows)
+        dx = torch.zeros_like(ws.dx)
+        args = (pot.precision, layout.rows, layout.ntiles, layout.t_tile_species.data_ptr(),
+                layout.t_tile_row.data_ptr(), C_ptr(pot.mlp.struct), ws.x.data_ptr(), _ptr(ws.x_lo))
+        tail = (e_rows.data_ptr(), dx.data_ptr(), ws.mlp_ws.data_ptr(), ws.mlp_ws.numel(), st)
+        if m is None:
+            call("fennol_mlp_energy_grad", *args, *tail)
+        else:
+            call("fennol_mlp_energy_grad_active", *args, m, *tail)
+        torch.cuda.synchronize()
+        outs[name] = (e_rows.cpu().numpy(), dx.cpu().numpy())
+    assert _err_word(pot) == 0
+    cols = np.concatenate([np.arange(64 * c, 64 * c + 64) for c in range(16) if (mask >> c) & 1])
+    np.testing.assert_allclose(outs["active"][0], outs["dense"][0], rtol=1e-6, atol=1e-7)
+    da, dd = outs["active"][1], outs["dense"][1]
+    np.testing.assert_allclose(da[:, cols], dd[:, cols], rtol=1e-5, atol=1e-7 * np.abs(dd).max())
+    inactive = np.setdiff1d(np.arange(da.shape[1]), cols)
+    assert not da[:, inactive].any()   # never written
