@@ -24,9 +24,10 @@ ERR_UNSUPPORTED = -3
 ERR_WORKSPACE = -4
 ERR_STATIC_LIMIT = -5
 
-STATUS_WORDS = 8
+STATUS_WORDS = 9
 ST_NBR_OVERFLOW, ST_NBR_MAXCOUNT, ST_FILTER_OVERFLOW, ST_FILTER_MAXCOUNT = 0, 1, 2, 3
 ST_ANG_OVERFLOW, ST_ANG_MAXCOUNT, ST_CELL_OVERFLOW, ST_REBUILD_COUNT = 4, 5, 6, 7
+ST_NONFINITE = 8
 
 PBC_NONE, PBC_MINIMUM_IMAGE, PBC_GENERAL = 0, 1, 2
 MAX_ANGULAR_NEIGHBORS = 96
@@ -50,6 +51,14 @@ class FennolError(RuntimeError):
     def __init__(self, fn: str, code: int):
         super().__init__(f"{fn} failed: {code} ({_ERRNAMES.get(code, 'unknown')})")
         self.code = code
+
+
+class NonFiniteError(FloatingPointError):
+    """A device check found a NaN or an infinity (status word ST_NONFINITE)."""
+
+
+class KernelTimeout(RuntimeError):
+    """A bounded wait inside the tensor-core MLP ran out (its error word was set)."""
 
 
 class AEVParams(C.Structure):
@@ -105,6 +114,9 @@ _SIGNATURES = {
     "fennol_md_step_systems": (I, [I, I, D, P, P, P, P, D, D, P, P, P, P, P, P, P, P, P, D, P, P]),
     "fennol_md_mark_rebuilt": (I, [I, P, P, P, P]),
     "fennol_md_kinetic": (I, [I, P, P, P, P]),
+    "fennol_check_finite": (I, [I, P, P, P, P, P]),
+    "fennol_mlp_wait_limit": (I, [D]),
+    "fennol_mlp_inject_stall": (I, [I]),
     "fennol_capture_if_begin": (I, [P, P, P]),
     "fennol_capture_if_end": (I, [P]),
 }
@@ -137,6 +149,19 @@ def load(path: Optional[os.PathLike] = None) -> C.CDLL:
     if path is None:
         _lib = lib
     return lib
+
+
+def check_finite(buffers, status, stream: int) -> None:
+    """Enqueue ``fennol_check_finite`` on up to four device tensors (float32
+    or float64): status[ST_NONFINITE] is set when one holds a NaN or an
+    infinity."""
+    bufs = [b for b in buffers if b is not None and b.numel() > 0]
+    k = len(bufs)
+    ptrs = (C.c_void_p * 4)(*[b.data_ptr() for b in bufs])
+    counts = (C.c_size_t * 4)(*[b.numel() for b in bufs])
+    dbl = (C.c_int * 4)(*[int(b.element_size() == 8) for b in bufs])
+    call("fennol_check_finite", k, C.cast(ptrs, C.c_void_p), C.cast(counts, C.c_void_p),
+         C.cast(dbl, C.c_void_p), status.data_ptr(), stream)
 
 
 def call(name: str, *args) -> int:

@@ -23,6 +23,7 @@ enum StatusWord {
   ST_ANG_MAXCOUNT = 5,    // largest angular neighbour count
   ST_CELL_OVERFLOW = 6,   // cell list inconsistency (should never be set)
   ST_REBUILD_COUNT = 7,   // number of neighbour rebuilds executed (MD)
+  ST_NONFINITE = 8,       // a checked buffer held a NaN or an infinity
 };
 
 // Packed periodic shift: three signed bytes (x | y<<8 | z<<16).

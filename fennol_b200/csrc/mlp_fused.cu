@@ -63,7 +63,11 @@ constexpr uint32_t kXStageWide = 6 * kAtom;       // 96 KB
 constexpr int kXStagesWide = 2;
 constexpr uint32_t kXpose = 8 * 32 * 32 * 4;      // per-epilogue-warp 32x32 dX staging tiles: 32 KB
 constexpr uint32_t kSmemMain = kActBytes + kWStages * kWStage + kXpose;  // 224 KB
+// bounded waits: default limit, and the settings of fennol_mlp_wait_limit /
+// fennol_mlp_inject_stall (host side)
 constexpr uint64_t kTimeoutNs = 2000000000ull;
+uint64_t g_wait_limit_ns = kTimeoutNs;
+int g_stall_launches = 0;
 
 struct FusedParams {
   int ntiles, n_models, n_species;
@@ -78,6 +82,8 @@ struct FusedParams {
   uint32_t xstage;
   float alpha, inv_models;
   unsigned long long kmask;  // active 64-column chunks of the input
+  unsigned long long timeout_ns;  // limit of every bounded wait
+  int stall;                      // the load producer issues no copies (timeout tests)
   const float4* scales;  // F16 forms: per group (s_W1, s_W2, s_W3, s_w4) powers of two
   const float* b1;
   const float* b2;
@@ -134,9 +140,10 @@ __device__ __forceinline__ void celu_pair(float z, float alpha, float inv_alpha,
 // Threads sleep in mbarrier.try_wait (woken when the phase completes) instead
 // of polling, so waiting epilogue warps do not take issue slots from the MMA
 // and TMA threads.
-__device__ __forceinline__ bool wait_bar(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* err) {
+__device__ __forceinline__ bool wait_bar(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* err,
+                                         uint64_t p_timeout_ns) {
   if (mbar_try(bar, parity, 20000u)) return true;
-  const uint64_t deadline = globaltimer() + kTimeoutNs;
+  const uint64_t deadline = globaltimer() + p_timeout_ns;
   while (true) {
     if (mbar_try(bar, parity, 20000u)) return true;
     if (*abort_flag) return false;
@@ -232,7 +239,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
 
   if (warp == 0) {
     // ------------------------------------------------------------------ TMA producer
-    if (lane == 0) {
+    // (with p.stall it issues nothing: the other roles' waits run out)
+    if (lane == 0 && !p.stall) {
       uint32_t xq = 0, wq = 0;
       int item = 0;
       bool ok = true;
@@ -241,12 +249,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
         const int sp = p.tile_species[w];
         for (int m = 0; m < M && ok; ++m, ++item) {
           const int g = m * p.n_species + sp;
-          if (item > 0 && !(ok = wait_bar(&bars->act_free, (item - 1) & 1, abort_flag, p.err))) break;
+          if (item > 0 && !(ok = wait_bar(&bars->act_free, (item - 1) & 1, abort_flag, p.err, p.timeout_ns))) break;
           for (unsigned long long rest = p.kmask; rest; rest &= rest - 1, ++xq) {
             const int kc = __ffsll((long long)rest) - 1;
             const int s = xq % XS;
             const uint32_t u = xq / XS;
-            if (u > 0 && !(ok = wait_bar(&bars->x_empty[s], (u - 1) & 1, abort_flag, p.err))) break;
+            if (u > 0 && !(ok = wait_bar(&bars->x_empty[s], (u - 1) & 1, abort_flag, p.err, p.timeout_ns))) break;
             uint8_t* st = act + s * p.xstage;
             mbar_expect_tx(&bars->x_full[s], x_tx);
             tma_load_2d(&maps.x, &bars->x_full[s], st, kc * BK, row0);
@@ -262,7 +270,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
             const int rs = XS - 1;
             if (xq > (uint32_t)rs) {
               const uint32_t last = xq - 1 - ((xq - 1 - rs) % XS);
-              if (!(ok = wait_bar(&bars->x_empty[rs], (last / XS) & 1, abort_flag, p.err))) break;
+              if (!(ok = wait_bar(&bars->x_empty[rs], (last / XS) & 1, abort_flag, p.err, p.timeout_ns))) break;
             }
           }
           // weight chunks of the remaining GEMMs, in MMA order
@@ -277,7 +285,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
               for (int t = 0; t < nt[jb]; ++t, ++wq) {
                 const int s = wq % kWStages;
                 const uint32_t u = wq / kWStages;
-                if (u > 0 && !(ok = wait_bar(&bars->w_empty[s], (u - 1) & 1, abort_flag, p.err))) break;
+                if (u > 0 && !(ok = wait_bar(&bars->w_empty[s], (u - 1) & 1, abort_flag, p.err, p.timeout_ns))) break;
                 mbar_expect_tx(&bars->w_full[s], (uint32_t)rows_g[jb] * BK * 2);
                 tma_load_2d(t ? wml[jb] : wm[jb], &bars->w_full[s], wring + s * kWStage, kc * BK, g * rows_g[jb]);
               }
@@ -289,7 +297,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
               for (int t = 0; t < 1 + p.wb_lo; ++t, ++wq) {
                 const int s = wq % kWStages;
                 const uint32_t u = wq / kWStages;
-                if (u > 0 && !(ok = wait_bar(&bars->w_empty[s], (u - 1) & 1, abort_flag, p.err))) break;
+                if (u > 0 && !(ok = wait_bar(&bars->w_empty[s], (u - 1) & 1, abort_flag, p.err, p.timeout_ns))) break;
                 mbar_expect_tx(&bars->w_full[s], (uint32_t)len * 64 * BK * 2);
                 for (int q = 0; q < len; ++q)
                   tma_load_2d(t ? &maps.w1_lo : &maps.w1, &bars->w_full[s], wring + s * kWStage + q * 64 * BK * 2,
@@ -304,11 +312,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
       int dummy = 0;
       for (uint32_t s = 0; s < (uint32_t)XS && s < xq; ++s) {
         const uint32_t last = xq - 1 - ((xq - 1 - s) % XS);
-        wait_bar(&bars->x_full[s], (last / XS) & 1, &dummy, p.err);
+        wait_bar(&bars->x_full[s], (last / XS) & 1, &dummy, p.err, p.timeout_ns);
       }
       for (uint32_t s = 0; s < (uint32_t)kWStages && s < wq; ++s) {
         const uint32_t last = wq - 1 - ((wq - 1 - s) % kWStages);
-        wait_bar(&bars->w_full[s], (last / kWStages) & 1, &dummy, p.err);
+        wait_bar(&bars->w_full[s], (last / kWStages) & 1, &dummy, p.err, p.timeout_ns);
       }
     }
   } else if (warp == 1) {
@@ -322,7 +330,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
       const uint32_t act_hi = smem_u32(act), act_lo = smem_u32(act + kActHalf);
       auto acquire_acc = [&](uint32_t b) -> bool {
         if (nuse[b] == 0) return true;
-        return wait_bar(&bars->acc_free[b], (nuse[b] - 1) & 1, abort_flag, p.err);
+        return wait_bar(&bars->acc_free[b], (nuse[b] - 1) & 1, abort_flag, p.err, p.timeout_ns);
       };
       // one GEMM whose A operand is the activation buffer (K/64 atoms) and B the
       // weight ring.  With wait_act, each K-atom is used as soon as the epilogue
@@ -333,11 +341,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
         const uint32_t d = tmem + b * 256;
         for (int kc = 0; kc < k / BK; ++kc) {
           if (wait_act) {
-            if (!wait_bar(&bars->act_ready[kc], act_phase[kc] & 1, abort_flag, p.err)) return false;
+            if (!wait_bar(&bars->act_ready[kc], act_phase[kc] & 1, abort_flag, p.err, p.timeout_ns)) return false;
             ++act_phase[kc];
           }
           int s = wq % kWStages;
-          if (!wait_bar(&bars->w_full[s], (wq / kWStages) & 1, abort_flag, p.err)) return false;
+          if (!wait_bar(&bars->w_full[s], (wq / kWStages) & 1, abort_flag, p.err, p.timeout_ns)) return false;
           fence_after_sync();
           uint32_t bs = smem_u32(wring + s * kWStage);
 #pragma unroll
@@ -350,7 +358,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
           ++wq;
           if (wlo) {
             s = wq % kWStages;
-            if (!wait_bar(&bars->w_full[s], (wq / kWStages) & 1, abort_flag, p.err)) return false;
+            if (!wait_bar(&bars->w_full[s], (wq / kWStages) & 1, abort_flag, p.err, p.timeout_ns)) return false;
             fence_after_sync();
             bs = smem_u32(wring + s * kWStage);
 #pragma unroll
@@ -373,7 +381,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
             int ki = 0;
             for (unsigned long long rest = p.kmask; rest; rest &= rest - 1, ++xq, ++ki) {
               const int s = xq % XS;
-              if (!(ok = wait_bar(&bars->x_full[s], (xq / XS) & 1, abort_flag, p.err))) break;
+              if (!(ok = wait_bar(&bars->x_full[s], (xq / XS) & 1, abort_flag, p.err, p.timeout_ns))) break;
               fence_after_sync();
               const uint32_t st = smem_u32(act + s * p.xstage);
 #pragma unroll
@@ -422,7 +430,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
       }
       // all issued MMAs complete before TMEM is released
       mma_commit(&bars->done);
-      wait_bar(&bars->done, 0, abort_flag, p.err);
+      wait_bar(&bars->done, 0, abort_flag, p.err, p.timeout_ns);
     }
   } else {
     // ------------------------------------------------------------------ epilogue
@@ -439,7 +447,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
     const bool with_lo = p.a_lo != 0;    // forward activations
     const bool grad_lo = p.g_lo != 0;    // input-gradient operands
     auto take_acc = [&](uint32_t b) -> bool {
-      bool ready = __all_sync(0xffffffffu, wait_bar(&bars->acc_full[b], nuse[b] & 1, abort_flag, p.err));
+      bool ready = __all_sync(0xffffffffu, wait_bar(&bars->acc_full[b], nuse[b] & 1, abort_flag, p.err, p.timeout_ns));
       if (ready) fence_after_sync();
       return ready;
     };
@@ -565,11 +573,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
           release_acc(b);
           if (half == 1) {
             // the previous row energies must have been read before they are overwritten
-            if (ex_phase > 0 && !(ok = wait_bar(&bars->ex_free, (ex_phase - 1) & 1, abort_flag, p.err))) break;
+            if (ex_phase > 0 && !(ok = wait_bar(&bars->ex_free, (ex_phase - 1) & 1, abort_flag, p.err, p.timeout_ns))) break;
             bars->ex[r] = e;
             mbar_arrive(&bars->ex_ready);
           } else {
-            if (!(ok = wait_bar(&bars->ex_ready, ex_phase & 1, abort_flag, p.err))) break;
+            if (!(ok = wait_bar(&bars->ex_ready, ex_phase & 1, abort_flag, p.err, p.timeout_ns))) break;
             e += bars->ex[r] + __ldg(p.b4 + g);
             mbar_arrive(&bars->ex_free);
             e_row += e * p.inv_models;
@@ -782,6 +790,12 @@ int fnl_mlp_fused(int precision, int rows, int ntiles, const int* tile_species, 
   p.e_rows = e_rows;
   p.dx = dx;
   p.err = (int*)ws;
+  p.timeout_ns = g_wait_limit_ns;
+  p.stall = 0;
+  if (g_stall_launches > 0) {
+    p.stall = 1;
+    --g_stall_launches;
+  }
   p.dc = (float*)((char*)ws + 256);
   const size_t smem = kSmemMain + sizeof(Bars) + 1024;
   static bool attr[2] = {false, false};
@@ -795,5 +809,17 @@ int fnl_mlp_fused(int precision, int rows, int ntiles, const int* tile_species, 
   const int grid = ntiles < sm_count() ? ntiles : sm_count();
   FNL_LAUNCH_PDL(kern, dim3(grid), dim3(kThreads), smem, st, maps, p);
   FNL_CHECK_LAUNCH();
+  return FENNOL_OK;
+}
+
+extern "C" int fennol_mlp_wait_limit(double seconds) {
+  if (!(seconds > 0.0) || seconds > 60.0) return FENNOL_ERR_INVALID;
+  g_wait_limit_ns = (uint64_t)(seconds * 1e9);
+  return FENNOL_OK;
+}
+
+extern "C" int fennol_mlp_inject_stall(int launches) {
+  if (launches < 0) return FENNOL_ERR_INVALID;
+  g_stall_launches = launches;
   return FENNOL_OK;
 }

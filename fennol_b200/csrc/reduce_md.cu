@@ -386,3 +386,54 @@ extern "C" int fennol_md_kinetic(int natoms, const double* v, const double* inv_
   FNL_CHECK_LAUNCH();
   return FENNOL_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Non-finite check of up to four buffers in one launch.
+// ---------------------------------------------------------------------------
+namespace {
+struct FiniteBufs {
+  const void* ptr[4];
+  unsigned long long count[4];
+  int is_double[4];
+  int n;
+};
+
+__global__ void k_check_finite(const FiniteBufs b, int* status) {
+  pdl_wait();
+  bool bad = false;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (int k = 0; k < b.n; ++k) {
+    const size_t n = b.count[k];
+    if (b.is_double[k]) {
+      const double* p = (const double*)b.ptr[k];
+      for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) bad |= !isfinite(p[i]);
+    } else {
+      const float* p = (const float*)b.ptr[k];
+      for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) bad |= !isfinite(p[i]);
+    }
+  }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(status + fnl::ST_NONFINITE, 1);
+}
+}  // namespace
+
+extern "C" int fennol_check_finite(int nbuf, const void* const* host_ptrs, const size_t* host_counts,
+                                   const int* host_is_double, int* status, void* stream) {
+  if (nbuf < 0 || nbuf > 4 || !status) return FENNOL_ERR_INVALID;
+  if (nbuf > 0 && (!host_ptrs || !host_counts || !host_is_double)) return FENNOL_ERR_INVALID;
+  FiniteBufs b{};
+  size_t total = 0;
+  for (int k = 0; k < nbuf; ++k) {
+    if (host_counts[k] > 0 && !host_ptrs[k]) return FENNOL_ERR_INVALID;
+    b.ptr[k] = host_ptrs[k];
+    b.count[k] = host_counts[k];
+    b.is_double[k] = host_is_double[k] != 0;
+    total = host_counts[k] > total ? host_counts[k] : total;
+  }
+  b.n = nbuf;
+  if (total == 0) return FENNOL_OK;
+  size_t blocks = (total + 255) / 256;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  FNL_LAUNCH_PDL(k_check_finite, dim3((unsigned)blocks), dim3(256), 0, (cudaStream_t)stream, b, status);
+  FNL_CHECK_LAUNCH();
+  return FENNOL_OK;
+}

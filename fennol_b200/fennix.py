@@ -922,6 +922,11 @@ class FENNIX:
         view = _RowsView(rows)
         pot.launch_forces(layout, view, ws, st, want_forces, want_virial)
         status = ws.status.cpu().numpy()
+        if pot.precision != _lib.MLP_FP32 and int(ws.mlp_ws[:4].view(torch.int32)[0]):
+            ws.mlp_ws[:4].view(torch.int32).zero_()
+            raise _lib.KernelTimeout("species MLP: a bounded wait inside the tensor-core kernel ran out")
+        if status[_lib.ST_NONFINITE]:
+            raise _lib.NonFiniteError("non-finite positions, energies or forces")
         if status[_lib.ST_ANG_OVERFLOW]:
             raise RuntimeError(f"more than {_lib.MAX_ANGULAR_NEIGHBORS} angular neighbours "
                                f"({int(status[_lib.ST_ANG_MAXCOUNT])}) around one atom")

@@ -90,6 +90,8 @@ class MDEngine:
         self.species = species
         self.cell = None if cell is None else np.asarray(cell, dtype=np.float64)
         coordinates = np.asarray(coordinates, dtype=np.float64)
+        if not np.all(np.isfinite(coordinates)):
+            raise ValueError("coordinates hold a NaN or an infinity")
         natoms = [species.shape[0]] if natoms is None else list(natoms)
         cells = None if cell is None else np.asarray(cell).reshape(-1, 3, 3)
         self.layout = pot.layout(species, natoms, cells, reach=pot.aev_cfg.radial_cutoff + float(skin))
@@ -195,7 +197,8 @@ class MDEngine:
             if self.verify_stride:
                 self.x_ref.copy_(self.x)  # the stream is torch's current one (captured or not)
         g.filter(lay, self.coords, ws.status, st)
-        self.pot.launch_forces(lay, g, ws, st, True)
+        # the finite check runs once per chunk (run), not every step
+        self.pot.launch_forces(lay, g, ws, st, True, check_finite=False)
 
     def launches_per_step(self) -> int:
         """Kernels of this library that one graph-replayed step without a
@@ -264,6 +267,12 @@ class MDEngine:
         self.step_count = n
         self.coords.copy_(self.x.to(torch.float32))
 
+    def check_finite(self):
+        """Enqueue the device check of positions, velocities and forces
+        (FeNNol's MD driver checks positions and velocities for NaN every
+        ``nsummary`` steps, ``md/dynamic.py:204-208, 595-597``)."""
+        _lib.check_finite([self.x, self.v, self.ws.forces4[:self.n]], self.ws.status, self._stream())
+
     def _regrow(self):
         grow = self.pot.check_status(self.ws, self.graph_buf)
         if grow is None:
@@ -295,7 +304,12 @@ class MDEngine:
                     rebuild = (self.step_count + k) % self.nblist_stride == 0
                     self._graph_for(bool(rebuild), 1).replay()
                     k += 1
-            if self._regrow():
+            self.check_finite()
+            try:
+                grown = self._regrow()
+            except _lib.NonFiniteError as err:
+                raise ValueError(f"dynamics crashed at step {self.step_count + chunk}.") from err
+            if grown:
                 continue  # replay the chunk with larger lists
             if self.displaced_beyond_skin():
                 self.shorten_stride()

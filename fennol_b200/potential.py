@@ -503,10 +503,14 @@ class ANIPotential:
     # --------------------------------------------------------------- launches
     def launch_forces(self, layout: BatchLayout, g: GraphBuffers, ws: Workspace, stream: int,
                       want_forces: bool = True, want_virial: bool = False,
-                      ghost_rows: Optional[torch.Tensor] = None):
+                      ghost_rows: Optional[torch.Tensor] = None, check_finite: bool = True):
         """AEV -> MLP -> energies (and adjoint -> forces) from the current radial
         list.  ``ghost_rows``: MLP rows of centres whose energy does not count
-        (their row energy and dE/dAEV are cleared before the sum and the adjoint)."""
+        (their row energy and dE/dAEV are cleared before the sum and the adjoint).
+        ``check_finite``: one more launch sets status[ST_NONFINITE] when the
+        positions, energies or forces hold a NaN or an infinity (an atom at a
+        NaN position drops out of every list, so the energy alone can stay
+        finite)."""
         lib_p = C_ptr(self.params)
         n = layout.n
         # the adjoint reuses the forward's staging when the buffers carry it
@@ -553,10 +557,25 @@ class ANIPotential:
                  layout.t_cell.data_ptr(), g.rad_j.data_ptr(), g.rad_s.data_ptr(), g.rad_n.data_ptr(),
                  g.cap_r, lib_p, layout.t_atom_row.data_ptr(), ws.dx.data_ptr(), ws.dx.shape[1],
                  ws.forces4.data_ptr(), ws.status.data_ptr(), stream)
+        if check_finite:
+            _lib.check_finite([ws.xyzs[:n], ws.energy, ws.forces4[:n] if want_forces else None], ws.status,
+                              stream)
 
     def check_status(self, ws: Workspace, g: GraphBuffers) -> Optional[Tuple[int, int]]:
-        """None if every list fitted, else the capacities to regrow to."""
+        """None if every list fitted, else the capacities to regrow to.
+        Raises :class:`NonFiniteError` on a NaN or infinity found by the
+        device check and :class:`KernelTimeout` when a bounded wait of the
+        tensor-core MLP ran out (its error word is cleared first, so the next
+        call starts clean)."""
         st = ws.status.cpu().numpy()
+        if self.precision != _lib.MLP_FP32:
+            err = ws.mlp_ws[:4].view(torch.int32)
+            if int(err[0]):
+                err.zero_()
+                raise _lib.KernelTimeout("species MLP: a bounded wait inside the tensor-core kernel ran out "
+                                         "(the launch was abandoned; its outputs are invalid)")
+        if st[_lib.ST_NONFINITE]:
+            raise _lib.NonFiniteError("non-finite positions, energies or forces")
         if st[_lib.ST_ANG_OVERFLOW]:
             raise RuntimeError(f"more than {_lib.MAX_ANGULAR_NEIGHBORS} angular neighbours "
                                f"({int(st[_lib.ST_ANG_MAXCOUNT])}) around one atom")
@@ -611,6 +630,10 @@ class ANIPotential:
         if natoms is None:
             natoms = [species.shape[0]]
         natoms = tuple(int(v) for v in np.asarray(natoms).reshape(-1))
+        if not (isinstance(coordinates, torch.Tensor) and coordinates.is_cuda):
+            # host input: checked before upload (device inputs by the device check)
+            if not np.all(np.isfinite(np.asarray(coordinates, dtype=np.float64))):
+                raise ValueError("coordinates hold a NaN or an infinity")
         if centres is not None:
             if len(natoms) != 1 or not 0 <= int(centres) <= natoms[0]:
                 raise ValueError("centres applies to a single system and must lie in [0, natoms]")

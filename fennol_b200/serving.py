@@ -81,6 +81,7 @@ class ServeResult:
     velocities: Optional[np.ndarray]   # A/ps, float64 (md: final velocities)
     arrival: float
     done: float
+    error: Optional[str] = None        # set when the request was refused (no other field is valid)
 
     @property
     def latency(self) -> float:
@@ -520,7 +521,13 @@ class ServingEngine:
             if t > timeout_s:
                 raise TimeoutError("serving loop did not finish")
             while pending and (not realtime or pending[0].arrival <= t):
-                waiting.append(pending.popleft())
+                r = pending.popleft()
+                if not np.all(np.isfinite(np.asarray(r.coordinates, dtype=np.float64))):
+                    # refused before admission, like a host-side input check
+                    self.results.append(ServeResult(r.rid, r.kind, r.natoms, float("nan"), None, None, None,
+                                                    r.arrival, now(), error="non-finite coordinates"))
+                    continue
+                waiting.append(r)
             progressed = self.ef.poll(now)
             progressed |= self.md.poll(now)
             if self.ef.inflight is None and waiting:
@@ -556,6 +563,8 @@ def atom_steps(results: Sequence[ServeResult], reqs: Dict[int, ServeRequest]) ->
     included)."""
     total = 0
     for r in results:
+        if r.error is not None:
+            continue
         q = reqs[r.rid]
         total += r.natoms * (1 + (q.md_steps if q.kind == "md" else 0))
     return total

@@ -36,7 +36,7 @@ extern "C" {
 #define FENNOL_ERR_WORKSPACE (-4)
 #define FENNOL_ERR_STATIC_LIMIT (-5) /* input larger than a fixed in-library scratch */
 
-#define FENNOL_STATUS_WORDS 8
+#define FENNOL_STATUS_WORDS 9
 #define FENNOL_ST_NBR_OVERFLOW 0
 #define FENNOL_ST_NBR_MAXCOUNT 1
 #define FENNOL_ST_FILTER_OVERFLOW 2
@@ -45,6 +45,7 @@ extern "C" {
 #define FENNOL_ST_ANG_MAXCOUNT 5
 #define FENNOL_ST_CELL_OVERFLOW 6
 #define FENNOL_ST_REBUILD_COUNT 7
+#define FENNOL_ST_NONFINITE 8        /* a checked buffer held a NaN or an infinity */
 
 /* Periodic handling of one system (GraphGenerator, preprocessing.py:117-258). */
 #define FENNOL_PBC_NONE 0
@@ -369,6 +370,22 @@ int fennol_mlp_energy_grad_active(int precision, int rows, int ntiles, const int
                                   const void* x_lo, unsigned long long active_chunks, float* e_rows,
                                   float* dx, void* workspace, size_t workspace_bytes, void* stream);
 
+/*
+ * Failure handling of the fused tensor-core MLP (no counterpart in the
+ * reference).  Every wait inside the kernel on a shared-memory barrier gives
+ * up after a time limit: the kernel then sets the int32 error word at the
+ * start of its workspace to 1, ends all its roles, frees its tensor memory
+ * and returns, so the context stays usable; the caller reads the word (and
+ * clears it) after the launch.  Host only.
+ *   fennol_mlp_wait_limit: the limit for later launches, in seconds
+ *     (0 < seconds <= 60; default 2).
+ *   fennol_mlp_inject_stall: the next `launches` fused launches start with a
+ *     load producer that issues no copies, so the waits of the other roles
+ *     run out (for tests of the timeout path; 0 clears).
+ */
+int fennol_mlp_wait_limit(double seconds);
+int fennol_mlp_inject_stall(int launches);
+
 /* ------------------------------------------------------------------------ */
 /* Reductions and outputs                                                    */
 /* ------------------------------------------------------------------------ */
@@ -460,6 +477,17 @@ int fennol_md_mark_rebuilt(int natoms, const double* x, double* x_ref, int* rebu
  */
 int fennol_capture_if_begin(void* stream, const int* flag, void* body_stream);
 int fennol_capture_if_end(void* body_stream);
+
+/*
+ * status[FENNOL_ST_NONFINITE] = 1 when any element of the nbuf (<= 4) device
+ * buffers is a NaN or an infinity; buffer k holds host_counts[k] float32
+ * (host_is_double[k] == 0) or float64 values.  One launch.  The host arrays
+ * are read during the call.  Plays the part of the reference MD driver's NaN
+ * check of positions and velocities (md/dynamic.py:204-208, 595-597), and
+ * also checks energies and forces of single points.
+ */
+int fennol_check_finite(int nbuf, const void* const* host_ptrs, const size_t* host_counts,
+                        const int* host_is_double, int* status, void* stream);
 
 /* kinetic[0] = 0.5 * sum m v^2 (float64, deterministic order). */
 int fennol_md_kinetic(int natoms, const double* v, const double* inv_mass, double* kinetic,
