@@ -301,6 +301,28 @@ def present_aev_columns(species, cfg) -> int:
     return s * cfg.radial_dist_divisions + s * (s + 1) // 2 * cfg.angular_sublength
 
 
+# products per GEMM of each tensor-core form: (forward, input gradient)
+PRODUCTS = {"bf16": (1, 1), "bf16x2": (2, 2), "bf16x3": (3, 3), "f16x3x1": (3, 1), "f16x3x2": (3, 2)}
+
+
+def mlp_work(pot, species, precision):
+    """FLOPs per atom and model: the dense count of SURVEY-style accounting
+    (1008 inputs), the count on the AEV columns that can be non-zero for
+    these species, and the MMA work the fused kernel issues (padded widths,
+    active 64-column input chunks, split products)."""
+    cols = present_aev_columns(species, pot.aev_cfg)
+    present = 2 * (cols * 256 + 256 * 192 + 192 * 160 + 160) * 2
+    out = {"dense_flop": MLP_FLOP_PER_ATOM, "present_column_flop": present, "present_columns": cols}
+    if precision in PRODUCTS:
+        pf, pb = PRODUCTS[precision]
+        mask = pot.active_chunks(int(np.bitwise_or.reduce(1 << np.unique(pot.aev_cfg.species_index(species)))))
+        k1 = 64 * bin(mask & 0xFFFF).count("1")
+        d1, d2, d3 = pot.mlp.dims[1:4]
+        out["mma_flop"] = 2 * (pf * (k1 * d1 + d1 * d2 + d2 * d3) + pb * (d3 * d2 + d2 * d1 + d1 * k1))
+        out["active_input_columns"] = k1
+    return out
+
+
 def rooflines(pot, eng, box, workload, precision, sm_mhz):
     """Per-kernel rooflines of the step's three large kernels.  The MLP is
     bound by the tensor pipe (algorithmic FLOPs against the sustained bf16
@@ -320,11 +342,22 @@ def rooflines(pot, eng, box, workload, precision, sm_mhz):
     aev_out = 2 if precision == "bf16" else 4
     fwd_bytes = n * (mean_nbr * 4 + 16 + cols * aev_out)
     clock_hz = (sm_mhz or 1965.0) * 1e6
+    work = mlp_work(pot, box.species, precision)
+    units = n * w["n_models"]
     kernels = {
         "mlp": {"kernel": "k_mlp_fused", "ms_per_launch": kt["mlp"], "bound": "tensor",
                 "algorithmic_flop_per_launch": flops, "achieved": flops / (kt["mlp"] * 1e-3) / 1e12,
-                "unit": "TFLOP/s", "peak": tf_sust, "peak_source": f"{src} bf16 sustained"},
+                "unit": "TFLOP/s", "peak": tf_sust, "peak_source": f"{src} bf16 sustained",
+                "flop_accounting": ("achieved = dense 1.352 MFLOP per atom and model (1008 inputs); "
+                                    "present_column_tflops counts only the AEV columns these species can "
+                                    "make non-zero; mma_tflops is the tensor-core work issued (padded "
+                                    "widths, active input chunks, split products)"),
+                "present_column_tflops": work["present_column_flop"] * units / (kt["mlp"] * 1e-3) / 1e12},
     }
+    if "mma_flop" in work:
+        mma = work["mma_flop"] * units / (kt["mlp"] * 1e-3) / 1e12
+        kernels["mlp"].update(mma_tflops=mma, mma_frac=mma / tf_sust,
+                              active_input_columns=work["active_input_columns"])
     for name, kname, b in (("aev_backward", "k_aev_backward", bwd_bytes), ("aev_forward", "k_aev_forward", fwd_bytes)):
         ms = kt[name]
         inst = profile_value("inst_per_launch", kname, workload)
