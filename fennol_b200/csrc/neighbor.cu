@@ -633,17 +633,48 @@ static __device__ __align__(256) unsigned char g_graph_scratch[kStaticScratchByt
 
 std::mutex g_scratch_mu;
 void* g_scratch_addr[kStaticMaxDevices] = {};
+unsigned long long g_scratch_ctx[kStaticMaxDevices] = {};
+
+// Unique id of the calling thread's current context (0 if none or if the
+// driver lacks cuCtxGetId): a context destroyed and created again, as by
+// cudaDeviceReset, has a new id, and device addresses of the old one are void.
+unsigned long long current_context_id() {
+  using GetCurrent = int (*)(void**);
+  using GetId = int (*)(void*, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrent>(p);
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetId>(p);
+  }
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current && get_id && get_current(&ctx) == 0 && ctx && get_id(ctx, &id) == 0) return id;
+  return 0;
+}
 
 // Device address of g_graph_scratch on the current device, looked up once
-// per device.  In host code the symbol itself is only a host-side stand-in.
+// per device and context (a new context, e.g. after cudaDeviceReset, is
+// looked up again).  In host code the symbol itself is only a host-side
+// stand-in.
 int scratch_address(void** out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kStaticMaxDevices) return FENNOL_ERR_CUDA;
   std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_addr[dev]) {
+  const unsigned long long ctx = current_context_id();
+  if (!g_scratch_addr[dev] || ctx != g_scratch_ctx[dev]) {
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_graph_scratch) != cudaSuccess || !p) return FENNOL_ERR_CUDA;
     g_scratch_addr[dev] = p;
+    g_scratch_ctx[dev] = current_context_id();  // the lookup may have created the context
   }
   *out = g_scratch_addr[dev];
   return FENNOL_OK;

@@ -124,7 +124,9 @@ int fennol_graph_build(const float* coords, int natoms, const int* atom_sys, int
  * FENNOL_ERR_STATIC_LIMIT and nothing is launched (see
  * fennol_graph_noalloc_limits).  The first call on a device looks up the
  * array's device address (cudaGetSymbolAddress); make that first call
- * before any stream capture.  All calls share the one array: calls whose
+ * before any stream capture.  The address is kept per device and context:
+ * after cudaDeviceReset (a new context) the next call looks it up again, so
+ * make that call outside stream capture too.  All calls share the one array: calls whose
  * work overlaps on the GPU (two streams, or two threads) race on it and must
  * be serialised by the caller.  Allocates nothing.
  */
