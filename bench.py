@@ -531,18 +531,15 @@ def step_line(workload, precision, device, steps, warmup, flush, bf16_weights=Fa
     return res
 
 
-DRIFT_OUTPUT_SCALE = 0.002
-
-
 def nve_drift(device, steps, workload="water98k", every=100, precision=DEFAULT_PRECISION):
-    """Total-energy record of an NVE run of the workload (float64
-    integrator): linear drift and largest excursion per atom.
+    """Total-energy record of an NVE run of the workload with the model the
+    throughput is timed on (last layer x0.02; float64 integrator): linear
+    drift and largest excursion per atom.  The random-weight network has no
+    repulsive core, so over thousands of steps its wells gather atoms; the
+    run stops early, saying so, if a list limit is hit."""
+    from fennol_b200.params import MD_OUTPUT_SCALE
 
-    The random-weight network has no repulsive core: over thousands of steps
-    its wells gather atoms.  The drift run therefore scales the last layer by
-    ``DRIFT_OUTPUT_SCALE`` (atomic energies well below kT), and stops early,
-    saying so, if a list limit is hit."""
-    box, pot, eng = make_engine(workload, precision, device, output_scale=DRIFT_OUTPUT_SCALE)
+    box, pot, eng = make_engine(workload, precision, device, output_scale=MD_OUTPUT_SCALE)
     n = box.natoms
     t_ps, etot = [], []
     done = 0
@@ -563,8 +560,7 @@ def nve_drift(device, steps, workload="water98k", every=100, precision=DEFAULT_P
     wall = time.perf_counter() - t0
     e = np.array(etot) / n
     slope = float(np.polyfit(np.array(t_ps), e, 1)[0]) if len(e) > 2 else 0.0
-    return {"workload": WORKLOADS[workload]["desc"] + f"; last layer x{DRIFT_OUTPUT_SCALE} for this run",
-            "precision": precision, "steps": done, "stopped": stopped, "dt_fs": eng.dt * 1000.0,
+    return {"workload": WORKLOADS[workload]["desc"], "precision": precision, "steps": done, "stopped": stopped, "dt_fs": eng.dt * 1000.0,
             "samples": len(e), "drift_kcalmol_atom_per_ns": slope * 1000.0,
             "max_abs_dev_kcalmol_atom": float(np.abs(e - e[0]).max()),
             "e0_kcalmol_atom": float(e[0]), "temperature_end_K": eng.temperature(),
@@ -676,8 +672,8 @@ def main():
                     help="headline, e2e and rooflines only (no comparisons, accuracy or side runs)")
     ap.add_argument("--skip-serving", action="store_true", help="skip the request-stream run")
     ap.add_argument("--skip-training", action="store_true", help="skip the training-gradient timing")
-    ap.add_argument("--nve-drift-steps", type=int, default=0,
-                    help="also record the NVE energy drift of the 98k-atom ensemble over this many steps")
+    ap.add_argument("--nve-drift-steps", type=int, default=10000,
+                    help="NVE energy-drift run of the 98k-atom ensemble on the MD model (0: skip)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

@@ -30,7 +30,7 @@ ST_ANG_OVERFLOW, ST_ANG_MAXCOUNT, ST_CELL_OVERFLOW, ST_REBUILD_COUNT = 4, 5, 6, 
 ST_NONFINITE = 8
 
 PBC_NONE, PBC_MINIMUM_IMAGE, PBC_GENERAL = 0, 1, 2
-MAX_ANGULAR_NEIGHBORS = 96
+MAX_ANGULAR_NEIGHBORS = 256
 
 AEV_F32, AEV_BF16, AEV_BF16X2, AEV_F16X2 = 0, 1, 2, 3
 MLP_FP32, MLP_BF16, MLP_BF16X2, MLP_BF16X3, MLP_F16X3X1, MLP_F16X3X2 = 0, 1, 2, 3, 4, 5

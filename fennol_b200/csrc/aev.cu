@@ -25,7 +25,11 @@ namespace {
 constexpr int kAevWarps = 8;
 constexpr int kMaxS = 8;
 constexpr int kMaxP = kMaxS * (kMaxS + 1) / 2;
-constexpr int kCapA = FENNOL_MAX_ANGULAR_NEIGHBORS;
+// Angular neighbours a centre's staging holds: the row capacity, at most
+// FENNOL_MAX_ANGULAR_NEIGHBORS.  A centre has no more angular neighbours than
+// radial ones, so rows of up to that capacity cannot overflow it.
+constexpr int kCapAMax = FENNOL_MAX_ANGULAR_NEIGHBORS;
+__host__ __device__ __forceinline__ int ang_cap(int cap) { return cap < kCapAMax ? cap : kCapAMax; }
 
 struct AevConst {
   int S, P, RD, AD, AS, F;
@@ -134,32 +138,35 @@ struct Stage {
   float4* tmp;   // [cap] (vx, vy, vz, d2) unsorted
   int* tkey;     // [cap] species | angular<<8
   float2* rd;    // [cap] radial (d, 0.25*fc) sorted by species
-  float4* au;    // [kCapA] angular (ux, uy, uz, d) sorted by species
-  float2* af;    // [kCapA] angular (fc, dfc)
-  int* aslot;    // [kCapA] radial row position of each angular neighbour
+  float4* au;    // [capa] angular (ux, uy, uz, d) sorted by species
+  float2* af;    // [capa] angular (fc, dfc)
+  int* aslot;    // [capa] radial row position of each angular neighbour
   int* cntw;     // [32] per-species counters
   int* rslot;    // [cap] radial row position of each sorted radial entry (tangent kernel only)
+  int capa;      // angular capacity, ang_cap(cap)
 };
 
 // `with_rd`: the sorted radial entries (d, 0.25 fc) are kept (forward and
 // tangent); the adjoint works from the unsorted rows and leaves them out.
 __host__ __device__ __forceinline__ size_t stage_bytes(int cap, bool with_rd = true) {
   // rounded to 16 bytes so that every per-warp carve-up keeps float4 alignment
-  return ((size_t)cap * (16 + 4 + (with_rd ? 8 : 0)) + (size_t)kCapA * (16 + 8 + 4) + 32 * 4 + 15) / 16 * 16;
+  return ((size_t)cap * (16 + 4 + (with_rd ? 8 : 0)) + (size_t)ang_cap(cap) * (16 + 8 + 4) + 32 * 4 + 15) / 16 * 16;
 }
 
 __device__ __forceinline__ Stage carve_stage(char* base, int cap, bool with_rd = true) {
   Stage st;
   st.tmp = (float4*)base;
   st.au = (float4*)(base + (size_t)cap * 16);
-  char* next = base + (size_t)cap * 16 + (size_t)kCapA * 16;
+  const int capa = ang_cap(cap);
+  char* next = base + (size_t)cap * 16 + (size_t)capa * 16;
   st.rd = with_rd ? (float2*)next : nullptr;
   if (with_rd) next += (size_t)cap * 8;
   st.af = (float2*)next;
-  st.tkey = (int*)((char*)st.af + (size_t)kCapA * 8);
+  st.tkey = (int*)((char*)st.af + (size_t)capa * 8);
   st.aslot = st.tkey + cap;
-  st.cntw = st.aslot + kCapA;
+  st.cntw = st.aslot + capa;
   st.rslot = nullptr;
+  st.capa = capa;
   return st;
 }
 
@@ -329,7 +336,7 @@ __device__ __forceinline__ void stage_row(const Stage& st, int* cntw, const floa
       float fc = d < K.rc ? 0.5f * cosf(d * K.pi_rc) + 0.5f : 0.f;
       if (kRd) st.rd[pos_r] = make_float2(d, 0.25f * fc);
       if (kRslot) st.rslot[pos_r] = k;
-      if (pos_a >= 0 && pos_a < kCapA) {
+      if (pos_a >= 0 && pos_a < st.capa) {
         float inv = 1.0f / fmaxf(d, 1e-5f);
         st.au[pos_a] = make_float4(v.x * inv, v.y * inv, v.z * inv, d);
         float sa, ca2;
@@ -467,13 +474,13 @@ k_aev_forward(const float4* __restrict__ xyzs, int n, const int* __restrict__ at
                   off_a, na);
   if (lane == 0) {
     status_max(status, ST_ANG_MAXCOUNT, na);
-    if (na > kCapA) status_set(status, ST_ANG_OVERFLOW);
+    if (na > st.capa) status_set(status, ST_ANG_OVERFLOW);
   }
   if (stage_g) {
     // the saved record uses the adjoint's layout (no sorted radial entries)
     char* rec = stage_g + (size_t)i * stage_bytes(cap, false);
     const Stage rs = carve_stage(rec, cap, false);
-    const int nac = min(na, kCapA);
+    const int nac = min(na, st.capa);
     for (int k = lane; k < cnt; k += 32) {
       rs.tmp[k] = st.tmp[k];
       rs.tkey[k] = st.tkey[k];
@@ -511,14 +518,14 @@ k_aev_forward(const float4* __restrict__ xyzs, int n, const int* __restrict__ at
   const unsigned present = __ballot_sync(0xffffffffu, lane < S && cnt_a > 0);
   for (unsigned m1 = present; m1; m1 &= m1 - 1) {
     const int s1 = __ffs(m1) - 1;
-    const int n1 = min(__shfl_sync(0xffffffffu, cnt_a, s1), kCapA);
+    const int n1 = min(__shfl_sync(0xffffffffu, cnt_a, s1), st.capa);
     const int o1 = __shfl_sync(0xffffffffu, off_a, s1);
     for (unsigned m2 = m1; m2; m2 &= m2 - 1) {
       const int s2 = __ffs(m2) - 1;
-      const int n2 = min(__shfl_sync(0xffffffffu, cnt_a, s2), kCapA);
+      const int n2 = min(__shfl_sync(0xffffffffu, cnt_a, s2), st.capa);
       const int o2 = __shfl_sync(0xffffffffu, off_a, s2);
       int T = s1 == s2 ? n1 * (n1 - 1) / 2 : n1 * n2;
-      if (o1 + n1 > kCapA || o2 + n2 > kCapA) T = 0;  // overflowing atom: reported above
+      if (o1 + n1 > st.capa || o2 + n2 > st.capa) T = 0;  // overflowing atom: reported above
       if (T == 0) continue;
       const int p = triu_pair(s1, s2, S);
       float acc[32];
@@ -608,13 +615,13 @@ k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ a
     const int* cw = in_record(rec, base, st.cntw);
     int na = 0;
     for (int s2 = 0; s2 < S; ++s2) na += cw[S + s2];
-    copy_stage(st, base, rec, cnt, min(na, kCapA), S, lane);
+    copy_stage(st, base, rec, cnt, min(na, st.capa), S, lane);
     __syncwarp();
   } else {
     int cnt_r, off_r, cnt_a, off_a, na;
     stage_row<true, false, false>(st, st.cntw, xyzs, pi, c, nbr_j, nbr_shift, row, cnt, K, lane, cnt_r, off_r,
                                   cnt_a, off_a, na);
-    if (na > kCapA && lane == 0) status_set(status, ST_ANG_OVERFLOW);
+    if (na > st.capa && lane == 0) status_set(status, ST_ANG_OVERFLOW);
   }
 
   // ---- radial: lane per neighbour (row order), gradient into gk[4k..4k+2]
@@ -658,14 +665,14 @@ k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ a
   if (lane == 0) {
     int nb = 0, tot = 0;
     for (int s1 = 0; s1 < S; ++s1) {
-      const int n1 = min(st.cntw[S + s1], kCapA);
+      const int n1 = min(st.cntw[S + s1], st.capa);
       const int o1 = st.cntw[3 * S + s1] - st.cntw[S + s1];  // running offset ended at off + count
       if (n1 == 0) continue;
       for (int s2 = s1; s2 < S; ++s2) {
-        const int n2 = min(st.cntw[S + s2], kCapA);
+        const int n2 = min(st.cntw[S + s2], st.capa);
         const int o2 = st.cntw[3 * S + s2] - st.cntw[S + s2];
         int T = s1 == s2 ? n1 * (n1 - 1) / 2 : n1 * n2;
-        if (o1 + n1 > kCapA || o2 + n2 > kCapA) T = 0;
+        if (o1 + n1 > st.capa || o2 + n2 > st.capa) T = 0;
         if (T == 0) continue;
         blk_cum[nb] = tot;
         blk_n[nb] = n1 | (n2 << 8) | ((s1 == s2) << 16);
@@ -859,7 +866,7 @@ k_aev_tangent(const float4* __restrict__ xyzs, int n, const int* __restrict__ at
   int cnt_r, off_r, cnt_a, off_a, na;
   stage_row<true, true>(st, st.cntw, xyzs, pi, c, nbr_j, nbr_shift, row, cnt, K, lane, cnt_r, off_r, cnt_a,
                         off_a, na);
-  if (na > kCapA && lane == 0) status_set(status, ST_ANG_OVERFLOW);
+  if (na > st.capa && lane == 0) status_set(status, ST_ANG_OVERFLOW);
 
   // per-neighbour tangents: d-dot = r.(u_j - u_i)/d and (u_j - u_i)/d
   for (int k = lane; k < cnt; k += 32) {
@@ -901,14 +908,14 @@ k_aev_tangent(const float4* __restrict__ xyzs, int n, const int* __restrict__ at
   const unsigned present = __ballot_sync(0xffffffffu, lane < S && cnt_a > 0);
   for (unsigned m1 = present; m1; m1 &= m1 - 1) {
     const int s1 = __ffs(m1) - 1;
-    const int n1 = min(__shfl_sync(0xffffffffu, cnt_a, s1), kCapA);
+    const int n1 = min(__shfl_sync(0xffffffffu, cnt_a, s1), st.capa);
     const int o1 = __shfl_sync(0xffffffffu, off_a, s1);
     for (unsigned m2 = m1; m2; m2 &= m2 - 1) {
       const int s2 = __ffs(m2) - 1;
-      const int n2 = min(__shfl_sync(0xffffffffu, cnt_a, s2), kCapA);
+      const int n2 = min(__shfl_sync(0xffffffffu, cnt_a, s2), st.capa);
       const int o2 = __shfl_sync(0xffffffffu, off_a, s2);
       int T = s1 == s2 ? n1 * (n1 - 1) / 2 : n1 * n2;
-      if (o1 + n1 > kCapA || o2 + n2 > kCapA) T = 0;
+      if (o1 + n1 > st.capa || o2 + n2 > st.capa) T = 0;
       if (T == 0) continue;
       const int p = triu_pair(s1, s2, S);
       float acc[32];

@@ -52,8 +52,11 @@ extern "C" {
 #define FENNOL_PBC_MINIMUM_IMAGE 1
 #define FENNOL_PBC_GENERAL 2
 
-/* Largest number of in-kernel angular neighbours per centre atom. */
-#define FENNOL_MAX_ANGULAR_NEIGHBORS 96
+/* Angular neighbours per centre atom that the AEV kernels stage on chip:
+ * the capacity of the radial rows they read, at most this value.  A centre
+ * has no more angular than radial neighbours, so rows of capacity up to 256
+ * never overflow it; longer rows report FENNOL_ST_ANG_OVERFLOW beyond 256. */
+#define FENNOL_MAX_ANGULAR_NEIGHBORS 256
 
 /* ------------------------------------------------------------------------ */
 /* Library                                                                   */

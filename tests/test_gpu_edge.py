@@ -72,3 +72,30 @@ def test_one_species_only(pot_tc):
     """Only carbon atoms: a single tile species, six networks unused."""
     mol = molecule_batch(1, seed=9, nmin=30, nmax=30)[0]
     check(pot_tc, mol.coordinates, np.full(mol.natoms, 6), [mol.natoms])
+
+
+def test_more_than_96_angular_neighbours(cuda_device):
+    """120 atoms inside a 1.7 A sphere: every atom has 119 angular neighbours
+    (the staging follows the row capacity, regrown from the first guess),
+    against the FP64 oracle."""
+    from fennol_b200.params import AEVConfig, MLPConfig
+    from fennol_b200.potential import ANIPotential, HARTREE_TO_KCALMOL
+    from oracle import ani_ref
+
+    rng = np.random.default_rng(5)
+    pts = []
+    while len(pts) < 120:
+        p = rng.uniform(-1.7, 1.7, 3)
+        if np.linalg.norm(p) < 1.7 and all(np.linalg.norm(p - q) > 0.15 for q in pts):
+            pts.append(p)
+    xyz = np.array(pts)
+    sp = rng.choice([1, 6, 8], size=120)
+    pot = ANIPotential(precision="fp32", device=cuda_device, seed=0)
+    e, f = pot.energy_and_forces(xyz, sp, [120])
+    layout, g, ws = next(iter(pot._cache.values()))
+    assert g.cap_r >= 119
+    r = ani_ref.energy_and_forces(xyz, sp, [120], pot.weights, AEVConfig(), MLPConfig())
+    de = abs(float(e[0]) - r["energy"][0]) * HARTREE_TO_KCALMOL / 120
+    scale = np.abs(r["forces"]).max()
+    assert de < 1e-3, de
+    np.testing.assert_allclose(f.cpu().numpy(), r["forces"], rtol=0, atol=1e-4 * scale)

@@ -6,8 +6,9 @@
   the slots must be distinct and inside that bound for any batch.
 * ``div_small`` (csrc/aev.cu) forms q = floor(v / n) from a float32
   reciprocal, (v + 1/2) * float32(1/n), for the triplet indices of the
-  adjoint (v < 96 * 96 + 96 * 2, n <= 96); it must be exact there without
-  its correction step (which stays in the kernel as a guard).
+  adjoint (v < 256 * 256 + 256 * 2, n <= 256, the largest angular staging);
+  it must be exact there without its correction step (which stays in the
+  kernel as a guard).
 """
 
 import numpy as np
@@ -46,9 +47,9 @@ def test_energy_slots_single_large_system():
 
 
 def test_div_small_exact_without_correction():
-    n = np.arange(1, 97, dtype=np.int64)
+    n = np.arange(1, 257, dtype=np.int64)
     rn = (np.float32(1.0) / n.astype(np.float32)).astype(np.float32)
-    v = np.arange(0, 96 * 96 + 2 * 96, dtype=np.int64)
+    v = np.arange(0, 256 * 256 + 2 * 256, dtype=np.int64)
     for k in range(n.size):
         q = ((v.astype(np.float32) + np.float32(0.5)) * rn[k]).astype(np.int64)  # float32 product, truncation
         np.testing.assert_array_equal(q, v // n[k])
