@@ -44,8 +44,11 @@ def triu_pair_index(num_species: int) -> np.ndarray:
 
 
 def celu(x: torch.Tensor, alpha: float) -> torch.Tensor:
-    """``jax.nn.celu``: ``x if x > 0 else alpha*expm1(x/alpha)``."""
-    return torch.where(x > 0, x, alpha * torch.expm1(x / alpha))
+    """``jax.nn.celu``: ``x if x > 0 else alpha*expm1(x/alpha)``, evaluated as
+    ``max(x, 0) + alpha*expm1(min(x, 0)/alpha)`` so that the exponential never
+    sees a large positive argument (a ``where`` over both branches would give
+    NaN gradients through the untaken branch for inputs above ~71)."""
+    return torch.clamp(x, min=0) + alpha * torch.expm1(torch.clamp(x, max=0) / alpha)
 
 
 class Graph:
