@@ -78,6 +78,13 @@ class MLPWeights(C.Structure):
                 ("f16_scale", C.c_void_p)]
 
 
+class NetTrain(C.Structure):
+    _fields_ = [("n_species", C.c_int), ("dims", C.c_int * 5), ("celu_alpha", C.c_float),
+                ("is_double", C.c_int),
+                ("w", (C.c_void_p * 8) * 4), ("b", (C.c_void_p * 8) * 4),
+                ("gw", (C.c_void_p * 8) * 4), ("gb", (C.c_void_p * 8) * 4)]
+
+
 P = C.c_void_p
 I = C.c_int
 D = C.c_double
@@ -115,6 +122,8 @@ _SIGNATURES = {
     "fennol_md_mark_rebuilt": (I, [I, P, P, P, P]),
     "fennol_md_kinetic": (I, [I, P, P, P, P]),
     "fennol_check_finite": (I, [I, P, P, P, P, P]),
+    "fennol_net_loss_grad_workspace_bytes": (SZ, [C.POINTER(NetTrain), P]),
+    "fennol_net_loss_grad": (I, [C.POINTER(NetTrain), P, P, P, P, I, P, P, SZ, P]),
     "fennol_mlp_wait_limit": (I, [D]),
     "fennol_mlp_inject_stall": (I, [I]),
     "fennol_capture_if_begin": (I, [P, P, P]),

@@ -18,12 +18,14 @@ same gradient is assembled from explicit pieces:
   ``sum_rows (dL/dE * E_row - <dE_row/dAEV_row, t_row>)`` with respect to
   every kernel and bias (CELU first and second derivatives included).
 
-The network part runs as plain GEMMs on the device (torch/cuBLAS), in
-float32 by default or float64.
+The network part is ``fennol_net_loss_grad`` (``csrc/train.cu``): grouped
+CUDA-core GEMMs and CELU kernels over all species of the batch, in float32
+by default or float64.
 """
 
 from __future__ import annotations
 
+import ctypes
 import dataclasses
 from typing import Dict, List, Tuple
 
@@ -42,48 +44,6 @@ class LossTerms:
     force_loss: float
     energy: np.ndarray   # [B] model unit
     forces: np.ndarray   # [N, 3]
-
-
-def _celu_parts(z: torch.Tensor, alpha: float):
-    """celu(z), celu'(z), celu''(z) as jax.nn.celu defines them (x > 0 branch)."""
-    pos = z > 0
-    ez = torch.exp(torch.clamp(z, max=0.0) / alpha)
-    h = torch.where(pos, z, alpha * (ez - 1.0))
-    d1 = torch.where(pos, torch.ones_like(z), ez)
-    d2 = torch.where(pos, torch.zeros_like(z), ez / alpha)
-    return h, d1, d2
-
-
-def network_loss_gradient(a: torch.Tensor, t: torch.Tensor, c_e: torch.Tensor, layers, alpha: float):
-    """Gradient with respect to ``layers`` [(W, b), ...] (torch, on device) of
-    ``sum_rows c_e[row] * f(a_row) - <grad_a f(a_row), t_row>`` for the
-    network ``f`` (CELU hidden layers, linear output of width 1)."""
-    n_hidden = len(layers) - 1
-    d1s, d2s, hs, zds, hds = [], [], [a], [], [t]
-    h, hd = a, t
-    for W, b in layers[:-1]:
-        z = h @ W + b
-        zd = hd @ W
-        h, d1, d2 = _celu_parts(z, alpha)
-        hd = d1 * zd
-        d1s.append(d1), d2s.append(d2), zds.append(zd)
-        hs.append(h), hds.append(hd)
-    W4, _ = layers[-1]
-    # seeds: energy output f -> c_e; tangent output s = hd_last . w4 -> -1
-    grads: List[Tuple[torch.Tensor, torch.Tensor]] = [None] * len(layers)
-    grads[-1] = (hs[-1].t() @ c_e[:, None] - hds[-1].sum(0)[:, None], c_e.sum().reshape(1))
-    hbar = c_e[:, None] * W4[:, 0][None, :]          # d/dh of the energy term
-    hdbar = -W4[:, 0][None, :].expand_as(hds[-1])    # d/dh-dot of the tangent term
-    for l in range(n_hidden - 1, -1, -1):
-        d1, d2, zd = d1s[l], d2s[l], zds[l]
-        zdbar = d1 * hdbar
-        zbar = d1 * hbar + d2 * zd * hdbar
-        W, _ = layers[l]
-        grads[l] = (hs[l].t() @ zbar + hds[l].t() @ zdbar, zbar.sum(0))
-        if l > 0:
-            hbar = zbar @ W.t()
-            hdbar = zdbar @ W.t()
-    return grads
 
 
 class LossGradient:
@@ -105,6 +65,30 @@ class LossGradient:
                        for sym, layers in pot.weights[0].items()}
         self.shapes = [tuple(t_.shape) for sym in pot.aev_cfg.species_order for wb in self.layers[sym]
                        for t_ in wb]
+        # the networks as fennol_net_loss_grad reads them; output pointers per call
+        order = pot.aev_cfg.species_order
+        net = _lib.NetTrain()
+        net.n_species = len(order)
+        dims = [self.layers[order[0]][0][0].shape[0]] + [w.shape[1] for w, _ in self.layers[order[0]]]
+        for k in range(5):
+            net.dims[k] = int(dims[k])
+        net.celu_alpha = pot.mlp_cfg.celu_alpha
+        net.is_double = int(dtype == torch.float64)
+        for s, sym in enumerate(order):
+            for l, (W, b) in enumerate(self.layers[sym]):
+                net.w[l][s] = W.data_ptr()
+                net.b[l][s] = b.data_ptr()
+        self.net = net
+        self.offsets = {}   # (species, layer) -> (kernel offset, bias offset) in the flat gradient
+        pos = 0
+        for s, sym in enumerate(order):
+            for l, (W, b) in enumerate(self.layers[sym]):
+                self.offsets[(s, l)] = (pos, pos + W.numel())
+                pos += W.numel() + b.numel()
+        self._ws = {}
+        self.path_description = ("CUDA E/F + AEV tangent kernel + fennol_net_loss_grad (grouped CUDA-core "
+                                 f"GEMMs and CELU kernels, {'float64' if net.is_double else 'float32'}), "
+                                 "one CUDA-graph replay per call from the third call on a batch")
         self.use_graphs = use_graphs
         self._rec = None      # captured pass of the current batch
         self._seen = None     # batch key of the previous call
@@ -130,28 +114,36 @@ class LossGradient:
         call("fennol_aev_tangent", ws.xyzs.data_ptr(), N, layout.t_atom_sys.data_ptr(), layout.t_cell.data_ptr(),
              g.rad_j.data_ptr(), g.rad_s.data_ptr(), g.rad_n.data_ptr(), g.cap_r, C_ptr(pot.params),
              layout.t_atom_row.data_ptr(), du4.data_ptr(), t.data_ptr(), d0, ws.status.data_ptr(), st)
-        F = pot.aev_cfg.aev_length
-        x = ws.x.float()
+        x = ws.x
         if ws.x_lo is not None:
-            x = x + ws.x_lo.float()
+            x = x.float() + ws.x_lo.float()
+        x = x.to(self.dtype).contiguous()
+        t = t.to(self.dtype).contiguous()
         # per-row energy seeds in the species-sorted row order of the AEV
         c_row = torch.zeros(layout.rows, dtype=self.dtype, device=dev)
         c_row[layout.t_atom_row.long()] = c_sys[layout.t_atom_sys.long()].to(self.dtype)
-        dev_grads: Dict[str, list] = {}
-        for k, row0, count in layout.species_segments:
-            sym = pot.aev_cfg.species_order[k]
-            sl = slice(row0, row0 + count)
-            dev_grads[sym] = network_loss_gradient(x[sl, :F].to(self.dtype), t[sl, :F].to(self.dtype),
-                                                   c_row[sl], self.layers[sym], pot.mlp_cfg.celu_alpha)
         out_small, out_grad = out
         torch.cat([ws.status.double(), torch.stack([self.w_e * (de ** 2).mean(), self.w_f * (df ** 2).mean()])],
                   out=out_small)
-        parts = []
-        for sym in pot.aev_cfg.species_order:
-            for l, (W, b) in enumerate(self.layers[sym]):
-                gW, gb = dev_grads[sym][l] if sym in dev_grads else (torch.zeros_like(W), torch.zeros_like(b))
-                parts += [gW.reshape(-1), gb.reshape(-1)]
-        torch.cat(parts, out=out_grad)
+        # the network sweep of every species present, straight into the flat gradient
+        S = self.net.n_species
+        row0 = np.zeros(S, np.int32)
+        rows = np.zeros(S, np.int32)
+        for k, r0, count in layout.species_segments:
+            row0[k], rows[k] = r0, count
+        net = self.net
+        base, esz = out_grad.data_ptr(), out_grad.element_size()
+        for (s, l), (ow, ob) in self.offsets.items():
+            net.gw[l][s] = base + ow * esz
+            net.gb[l][s] = base + ob * esz
+        out_grad.zero_()
+        key = rows.tobytes()
+        if key not in self._ws:
+            nb = _lib.load().fennol_net_loss_grad_workspace_bytes(ctypes.byref(net), rows.ctypes.data)
+            self._ws = {key: torch.empty(max(int(nb), 256), dtype=torch.uint8, device=dev)}
+        wsb = self._ws[key]
+        call("fennol_net_loss_grad", ctypes.byref(net), row0.ctypes.data, rows.ctypes.data, x.data_ptr(),
+             t.data_ptr(), d0, c_row.data_ptr(), wsb.data_ptr(), wsb.numel(), st)
 
     def __call__(self, coordinates, species, natoms, e_ref, f_ref, cells=None):
         pot, dev = self.pot, self.pot.device

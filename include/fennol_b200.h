@@ -392,6 +392,49 @@ int fennol_mlp_wait_limit(double seconds);
 int fennol_mlp_inject_stall(int launches);
 
 /* ------------------------------------------------------------------------ */
+/* Training-loss gradient                                                    */
+/* ------------------------------------------------------------------------ */
+
+/*
+ * One species network per species, as the training gradient reads it
+ * (unpadded FullyConnectedNet layers, misc/nets.py:13-102):
+ *   w[l][s]: kernel [dims[l]][dims[l+1]] row-major, b[l][s]: bias [dims[l+1]];
+ *   gw[l][s], gb[l][s]: outputs, same layouts.  dims = 1008, 256, 192, 160, 1
+ *   for ANI-2x (dims[4] must be 1).  is_double selects float64 buffers and
+ *   arithmetic, otherwise float32.  Pointers of species without rows may be NULL.
+ */
+typedef struct fennol_net_train {
+  int n_species; /* <= 8 */
+  int dims[5];
+  float celu_alpha;
+  int is_double;
+  const void* w[FENNOL_MLP_LAYERS][8];
+  const void* b[FENNOL_MLP_LAYERS][8];
+  void* gw[FENNOL_MLP_LAYERS][8];
+  void* gb[FENNOL_MLP_LAYERS][8];
+} fennol_net_train;
+
+/* Workspace of fennol_net_loss_grad for host_rows[s] rows per species, in bytes. */
+size_t fennol_net_loss_grad_workspace_bytes(const fennol_net_train* net, const int* host_rows);
+
+/*
+ * Network part of the training-loss parameter gradient.  Replaces the
+ * network half of jax.value_and_grad over a loss with forces
+ * (training/utils.py:140-525, :508): for each species s, the gradient with
+ * respect to its kernels and biases of
+ *     sum over its rows r of  c_row[r] f_s(x_r) - <grad f_s(x_r), t_r>,
+ * where x (AEV rows) and t (their tangents along dL/dF, fennol_aev_tangent)
+ * are [rows][ld] in the species-sorted layout, species s owning rows
+ * [host_row0[s], host_row0[s] + host_rows[s]), and c_row[r] = dL/dE of row r's
+ * system.  CELU first and second derivatives are included.  All buffers in
+ * the sweep's type (float32 or float64); workspace 256-byte aligned.  Each
+ * stage is one grouped launch over the species; no host synchronisation.
+ */
+int fennol_net_loss_grad(const fennol_net_train* net, const int* host_row0, const int* host_rows,
+                         const void* x, const void* t, int ld, const void* c_row, void* workspace,
+                         size_t workspace_bytes, void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* Reductions and outputs                                                    */
 /* ------------------------------------------------------------------------ */
 
