@@ -19,15 +19,19 @@
 // The activation and its tangent of a species are stacked in one [2R x d]
 // buffer, so every product above is one plain GEMM; all species of a batch
 // go through one grouped launch per stage (blockIdx.z = species).  GEMMs are
-// 64 x 64 shared-memory tiles with 4 x 4 register blocks, float32 or float64
-// arithmetic (the sweep's precision); sums over rows are fixed-order, so the
-// result is deterministic.
+// 128 x 128 shared-memory tiles with 8 x 8 register blocks, float32 or
+// float64 arithmetic (the sweep's precision); the weight-gradient products
+// (K = all rows of a species) are split along K with the partial products
+// summed in a fixed order, so the result is deterministic.
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace {
 
 constexpr int kMaxG = 8;   // species per batch
-constexpr int BM = 64, BN = 64, BK = 16;
+constexpr int BM = 128, BN = 128, BK = 8;
+constexpr int kMaxSplit = 8;   // K slices of one GEMM (partials summed in order)
 
 template <typename T>
 struct GemmGroups {
@@ -35,90 +39,130 @@ struct GemmGroups {
   const T* b[kMaxG];
   T* c[kMaxG];
   const T* bias[kMaxG];
+  T* part[kMaxG];   // [splits][m][n] partial products when splits > 1
   int m[kMaxG], k[kMaxG], lda[kMaxG], ldb[kMaxG], ldc[kMaxG], bias_rows[kMaxG];
+  int splits;
 };
+
+template <typename T>
+__device__ __forceinline__ void lds4(const T* p, T* v) {
+  if constexpr (sizeof(T) == 4) {
+    const float4 q = *reinterpret_cast<const float4*>(p);
+    v[0] = q.x, v[1] = q.y, v[2] = q.z, v[3] = q.w;
+  } else {
+    const double2 q0 = *reinterpret_cast<const double2*>(p);
+    const double2 q1 = *reinterpret_cast<const double2*>(p + 2);
+    v[0] = q0.x, v[1] = q0.y, v[2] = q1.x, v[3] = q1.y;
+  }
+}
 
 // C[m][n] = sum_k op(A)[m][k] op(B)[k][n] (+ bias[n] for m < bias_rows);
 // op(A) = A[k][m] when TA (A stored k-major), A[m][k] otherwise; op(B) =
-// B[n][k] when TB, B[k][n] otherwise.
+// B[n][k] when TB, B[k][n] otherwise.  128 x 128 tiles, 256 threads with an
+// 8 x 8 register block each (rows ty*4 and 64 + ty*4, columns tx*4 and
+// 64 + tx*4), the next K-slice prefetched into registers while the current
+// one is multiplied.  blockIdx.z = group * splits + split; with splits > 1
+// each split writes its partial product and k_split_sum adds them in order.
 template <typename T, bool TA, bool TB>
 __global__ void __launch_bounds__(256) k_gemm(const GemmGroups<T> g, int N) {
-  const int grp = blockIdx.z;
+  const int grp = blockIdx.z / g.splits, split = blockIdx.z % g.splits;
   const int M = g.m[grp], K = g.k[grp];
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
   if (m0 >= M) return;
+  const int kper = ((K + g.splits - 1) / g.splits + BK - 1) / BK * BK;
+  const int kb = split * kper, ke = min(K, kb + kper);
   const T* __restrict__ A = g.a[grp];
   const T* __restrict__ B = g.b[grp];
   const int lda = g.lda[grp], ldb = g.ldb[grp];
-  __shared__ T As[BK][BM + 4];
-  __shared__ T Bs[BK][BN + 4];
+  __shared__ __align__(16) T As[2][BK][BM];
+  __shared__ __align__(16) T Bs[2][BK][BN];
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  T acc[4][4];
+  // element e = tid + 256 i (i < 4) of a BK x 128 slice
+  auto fetch = [&](int k0, T* ra, T* rb) {
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
-  for (int k0 = 0; k0 < K; k0 += BK) {
-#pragma unroll
-    for (int e = tid; e < BM * BK; e += 256) {
+    for (int i = 0; i < 4; ++i) {
+      const int e = tid + 256 * i;
       int mm, kk;
-      if (TA) {
-        mm = e % BM;
-        kk = e / BM;
-      } else {
-        kk = e % BK;
-        mm = e / BK;
-      }
+      if (TA) { mm = e % BM; kk = e / BM; } else { kk = e % BK; mm = e / BK; }
       const int m = m0 + mm, k = k0 + kk;
-      T v = T(0);
-      if (m < M && k < K) v = TA ? A[(size_t)k * lda + m] : A[(size_t)m * lda + k];
-      As[kk][mm] = v;
+      ra[i] = (m < M && k < ke) ? (TA ? A[(size_t)k * lda + m] : A[(size_t)m * lda + k]) : T(0);
+      int nn;
+      if (TB) { kk = e % BK; nn = e / BK; } else { nn = e % BN; kk = e / BN; }
+      const int n = n0 + nn, k2 = k0 + kk;
+      rb[i] = (n < N && k2 < ke) ? (TB ? B[(size_t)n * ldb + k2] : B[(size_t)k2 * ldb + n]) : T(0);
     }
+  };
+  auto store = [&](int buf, const T* ra, const T* rb) {
 #pragma unroll
-    for (int e = tid; e < BN * BK; e += 256) {
-      int nn, kk;
-      if (TB) {
-        kk = e % BK;
-        nn = e / BK;
-      } else {
-        nn = e % BN;
-        kk = e / BN;
-      }
-      const int n = n0 + nn, k = k0 + kk;
-      T v = T(0);
-      if (n < N && k < K) v = TB ? B[(size_t)n * ldb + k] : B[(size_t)k * ldb + n];
-      Bs[kk][nn] = v;
+    for (int i = 0; i < 4; ++i) {
+      const int e = tid + 256 * i;
+      if (TA) As[buf][e / BM][e % BM] = ra[i]; else As[buf][e % BK][e / BK] = ra[i];
+      if (TB) Bs[buf][e % BK][e / BK] = rb[i]; else Bs[buf][e / BN][e % BN] = rb[i];
     }
-    __syncthreads();
+  };
+  T acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = T(0);
+  T ra[4], rb[4];
+  int buf = 0;
+  if (kb < ke) {
+    fetch(kb, ra, rb);
+    store(0, ra, rb);
+  }
+  __syncthreads();
+  for (int k0 = kb; k0 < ke; k0 += BK) {
+    const bool more = k0 + BK < ke;
+    if (more) fetch(k0 + BK, ra, rb);
 #pragma unroll
     for (int kk = 0; kk < BK; ++kk) {
-      T a[4], b[4];
+      T a[8], b[8];
+      lds4(&As[buf][kk][ty * 4], a);
+      lds4(&As[buf][kk][64 + ty * 4], a + 4);
+      lds4(&Bs[buf][kk][tx * 4], b);
+      lds4(&Bs[buf][kk][64 + tx * 4], b + 4);
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
+      for (int i = 0; i < 8; ++i)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx * 4 + j];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * b[j];
+        for (int j = 0; j < 8; ++j) acc[i][j] += a[i] * b[j];
     }
+    if (more) store(buf ^ 1, ra, rb);
     __syncthreads();
+    buf ^= 1;
   }
-  T* __restrict__ C = g.c[grp];
-  const T* bias = g.bias[grp];
-  const int ldc = g.ldc[grp], brows = g.bias_rows[grp];
+  const bool partial = g.splits > 1;
+  T* __restrict__ C = partial ? g.part[grp] + (size_t)split * M * N : g.c[grp];
+  const int ldc = partial ? N : g.ldc[grp];
+  const T* bias = partial ? nullptr : g.bias[grp];
+  const int brows = g.bias_rows[grp];
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int m = m0 + ty * 4 + i;
+  for (int i = 0; i < 8; ++i) {
+    const int m = m0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + i - 4);
     if (m >= M) continue;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int n = n0 + tx * 4 + j;
+    for (int j = 0; j < 8; ++j) {
+      const int n = n0 + (j < 4 ? tx * 4 + j : 64 + tx * 4 + j - 4);
       if (n >= N) continue;
       T v = acc[i][j];
       if (bias && m < brows) v += bias[n];
       C[(size_t)m * ldc + n] = v;
     }
+  }
+}
+
+// C = sum over splits of the partial products, in split order (+ bias)
+template <typename T>
+__global__ void k_split_sum(const GemmGroups<T> g, int N) {
+  const int grp = blockIdx.y;
+  const int M = g.m[grp];
+  const size_t total = (size_t)M * N;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const int m = (int)(i / N), n = (int)(i % N);
+    T v = T(0);
+    for (int s = 0; s < g.splits; ++s) v += g.part[grp][(size_t)s * total + i];
+    if (g.bias[grp] && m < g.bias_rows[grp]) v += g.bias[grp][n];
+    g.c[grp][(size_t)m * g.ldc[grp] + n] = v;
   }
 }
 
@@ -241,17 +285,28 @@ inline dim3 egrid(size_t total, int groups) {
   return dim3((unsigned)b, (unsigned)groups);
 }
 
+// One grouped GEMM launch; with splits > 1 the caller has set g.part and the
+// partial products are summed in split order by a second launch.
 template <typename T, bool TA, bool TB>
-int gemm(const GemmGroups<T>& g, int ng, int N, int Mmax, cudaStream_t st) {
+int gemm(GemmGroups<T> g, int ng, int N, int Mmax, int splits, cudaStream_t st) {
   if (ng == 0 || N <= 0 || Mmax <= 0) return FENNOL_OK;
-  dim3 grid((N + BN - 1) / BN, (Mmax + BM - 1) / BM, ng);
+  g.splits = splits;
+  dim3 grid((N + BN - 1) / BN, (Mmax + BM - 1) / BM, ng * splits);
   k_gemm<T, TA, TB><<<grid, 256, 0, st>>>(g, N);
+  if (splits > 1) k_split_sum<T><<<egrid((size_t)Mmax * N, ng), 256, 0, st>>>(g, N);
   return cudaGetLastError() == cudaSuccess ? FENNOL_OK : FENNOL_ERR_CUDA;
+}
+
+// K slices of the weight-gradient products (K = 2R rows): enough blocks to
+// fill the SMs, at least 512 rows per slice
+inline int splits_for(int kmax) {
+  int s = (kmax + 511) / 512;
+  return s < 1 ? 1 : (s > kMaxSplit ? kMaxSplit : s);
 }
 
 // workspace carve-up of one species with R rows (elements of T)
 struct Carve {
-  size_t h0, z[4], h[4], zb[4], hb[4], v, total;
+  size_t h0, z[4], h[4], zb[4], hb[4], v, part, total;
 };
 
 Carve carve(const int* dims, int R) {
@@ -271,6 +326,9 @@ Carve carve(const int* dims, int R) {
   }
   for (int l = 1; l <= 2; ++l) c.hb[l] = take(R2 * dims[l]);
   c.v = take(R2);
+  size_t mn = 0;
+  for (int l = 1; l <= 4; ++l) mn = std::max(mn, (size_t)dims[l - 1] * dims[l]);
+  c.part = take((size_t)kMaxSplit * mn);
   c.total = o;
   return c;
 }
@@ -329,7 +387,7 @@ int run(const fennol_net_train* net, const int* host_row0, const int* host_rows,
       g.ldc[gi] = d[l];
       g.bias_rows[gi] = R;
     }
-    if ((rc = gemm<T, false, false>(g, ng, d[l], 2 * Rmax, st))) return rc;
+    if ((rc = gemm<T, false, false>(g, ng, d[l], 2 * Rmax, 1, st))) return rc;
     Elem<T> e{};
     for (int gi = 0; gi < ng; ++gi) {
       e.in0[gi] = base[gi] + cv[gi].z[l];
@@ -357,13 +415,14 @@ int run(const fennol_net_train* net, const int* host_row0, const int* host_rows,
       g.a[gi] = base[gi] + cv[gi].h[3];
       g.b[gi] = base[gi] + cv[gi].v;
       g.c[gi] = (T*)net->gw[3][sp[gi]];
+      g.part[gi] = base[gi] + cv[gi].part;
       g.m[gi] = d[3];
       g.k[gi] = 2 * R;
       g.lda[gi] = d[3];
       g.ldb[gi] = 1;
       g.ldc[gi] = 1;
     }
-    if ((rc = gemm<T, true, false>(g, ng, 1, d[3], st))) return rc;
+    if ((rc = gemm<T, true, false>(g, ng, 1, d[3], splits_for(2 * Rmax), st))) return rc;
     // grad b4 = sum of c_e over the species' rows
     Elem<T> c{};
     for (int gi = 0; gi < ng; ++gi) {
@@ -382,13 +441,14 @@ int run(const fennol_net_train* net, const int* host_row0, const int* host_rows,
       g.a[gi] = base[gi] + (l == 1 ? cv[gi].h0 : cv[gi].h[l - 1]);
       g.b[gi] = base[gi] + cv[gi].zb[l];
       g.c[gi] = (T*)net->gw[l - 1][sp[gi]];
+      g.part[gi] = base[gi] + cv[gi].part;
       g.m[gi] = d[l - 1];
       g.k[gi] = 2 * R;
       g.lda[gi] = d[l - 1];
       g.ldb[gi] = d[l];
       g.ldc[gi] = d[l];
     }
-    if ((rc = gemm<T, true, false>(g, ng, d[l], d[l - 1], st))) return rc;
+    if ((rc = gemm<T, true, false>(g, ng, d[l], d[l - 1], splits_for(2 * Rmax), st))) return rc;
     Elem<T> c{};
     for (int gi = 0; gi < ng; ++gi) {
       c.in0[gi] = base[gi] + cv[gi].zb[l];
@@ -410,7 +470,7 @@ int run(const fennol_net_train* net, const int* host_row0, const int* host_rows,
       h.ldb[gi] = d[l];
       h.ldc[gi] = d[l - 1];
     }
-    if ((rc = gemm<T, false, true>(h, ng, d[l - 1], 2 * Rmax, st))) return rc;
+    if ((rc = gemm<T, false, true>(h, ng, d[l - 1], 2 * Rmax, 1, st))) return rc;
     Elem<T> e{};
     for (int gi = 0; gi < ng; ++gi) {
       e.in0[gi] = base[gi] + cv[gi].hb[l - 1];

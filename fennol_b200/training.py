@@ -202,7 +202,12 @@ class LossGradient:
         """Loss terms and the gradient as views into one host copy of the flat
         device gradient (float64 arrays for float64 sweeps, else float32)."""
         l_e, l_f = float(small[_lib.STATUS_WORDS]), float(small[_lib.STATUS_WORDS + 1])
-        host = grad_dev.cpu().numpy()
+        # one copy into a pinned buffer; the arrays returned are copies of it
+        if getattr(self, "_host", None) is None or self._host.shape != grad_dev.shape or \
+                self._host.dtype != grad_dev.dtype:
+            self._host = torch.empty(grad_dev.shape, dtype=grad_dev.dtype, pin_memory=True)
+        self._host.copy_(grad_dev)
+        host = self._host.numpy().copy()
         grads: Dict[str, List[Tuple[np.ndarray, np.ndarray]]] = {}
         pos, i = 0, 0
         for sym in self.pot.aev_cfg.species_order:
