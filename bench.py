@@ -814,6 +814,8 @@ def main():
             res["water12k"] = c2
         if not args.skip_serving:
             res["serving"] = serving_run(device)
+            # below saturation the latencies measure service, not queueing
+            res["serving_500rps"] = serving_run(device, rate_hz=500.0)
         if not args.skip_training:
             res["training_256mol"] = training_256(device)
         if args.nve_drift_steps > 0:
