@@ -657,8 +657,8 @@ k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ a
   // Block table, built once per centre so that a triplet needs no per-species
   // lookups: first triplet, sizes, offsets, pair index, 1/n of each block.
   int* blk_cum = blkw;                                   // [kMaxBlk + 2]: first triplet, end, count
-  int* blk_n = blkw + kMaxBlk + 2;                       // n1 | n2 << 8 | (s1 == s2) << 16
-  int* blk_o = blk_n + kMaxBlk;                          // o1 | o2 << 8
+  int* blk_n = blkw + kMaxBlk + 2;                       // n1 | n2 << 12 | (s1 == s2) << 24
+  int* blk_o = blk_n + kMaxBlk;                          // o1 | o2 << 12 (counts and offsets <= 256)
   int* blk_p = blk_o + kMaxBlk;                          // species-pair index
   float* blk_r1 = reinterpret_cast<float*>(blk_p + kMaxBlk);  // 1 / n1
   float* blk_r2 = blk_r1 + kMaxBlk;                           // 1 / n2
@@ -675,8 +675,8 @@ k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ a
         if (o1 + n1 > st.capa || o2 + n2 > st.capa) T = 0;
         if (T == 0) continue;
         blk_cum[nb] = tot;
-        blk_n[nb] = n1 | (n2 << 8) | ((s1 == s2) << 16);
-        blk_o[nb] = o1 | (o2 << 8);
+        blk_n[nb] = n1 | (n2 << 12) | ((s1 == s2) << 24);
+        blk_o[nb] = o1 | (o2 << 12);
         blk_p[nb] = triu_pair(s1, s2, S);
         blk_r1[nb] = 1.0f / (float)n1;
         blk_r2[nb] = 1.0f / (float)n2;
@@ -695,16 +695,16 @@ k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ a
     while (k + 1 < nblk && blk_cum[k + 1] <= t) ++k;
     const int tl = t - blk_cum[k];
     const int nn = blk_n[k], oo = blk_o[k];
-    const int n1 = nn & 0xFF, n2 = (nn >> 8) & 0xFF;
-    const int o1 = oo & 0xFF, o2 = oo >> 8;
+    const int n1 = nn & 0xFFF, n2 = (nn >> 12) & 0xFFF;
+    const int o1 = oo & 0xFFF, o2 = oo >> 12;
     int a, b;
-    if (nn >> 16) {
+    if (nn >> 24) {
       diag_ab(tl, n1, a, b);
       a += o1;
       b += o1;
     } else {
       // aa = tl mod n1, dd = tl div n1, b = o2 + (aa + dd) mod n2, as exact
-      // quotients through 1/n (n <= 96, tl < 96 * 96)
+      // quotients through 1/n (n <= 256, tl < 256 * 256)
       int dd, aa, bb;
       div_small(tl, n1, blk_r1[k], dd, aa);
       int q2;

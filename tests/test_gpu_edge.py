@@ -74,10 +74,12 @@ def test_one_species_only(pot_tc):
     check(pot_tc, mol.coordinates, np.full(mol.natoms, 6), [mol.natoms])
 
 
-def test_more_than_96_angular_neighbours(cuda_device):
+@pytest.mark.parametrize("elements", [(1, 6, 8), (6,)])
+def test_more_than_96_angular_neighbours(cuda_device, elements):
     """120 atoms inside a 1.7 A sphere: every atom has 119 angular neighbours
     (the staging follows the row capacity, regrown from the first guess),
-    against the FP64 oracle."""
+    three species or one (a single 119-neighbour block), against the FP64
+    oracle."""
     from fennol_b200.params import AEVConfig, MLPConfig
     from fennol_b200.potential import ANIPotential, HARTREE_TO_KCALMOL
     from oracle import ani_ref
@@ -89,7 +91,7 @@ def test_more_than_96_angular_neighbours(cuda_device):
         if np.linalg.norm(p) < 1.7 and all(np.linalg.norm(p - q) > 0.15 for q in pts):
             pts.append(p)
     xyz = np.array(pts)
-    sp = rng.choice([1, 6, 8], size=120)
+    sp = rng.choice(list(elements), size=120)
     pot = ANIPotential(precision="fp32", device=cuda_device, seed=0)
     e, f = pot.energy_and_forces(xyz, sp, [120])
     layout, g, ws = next(iter(pot._cache.values()))
