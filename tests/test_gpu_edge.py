@@ -99,5 +99,7 @@ def test_more_than_96_angular_neighbours(cuda_device, elements):
     r = ani_ref.energy_and_forces(xyz, sp, [120], pot.weights, AEVConfig(), MLPConfig())
     de = abs(float(e[0]) - r["energy"][0]) * HARTREE_TO_KCALMOL / 120
     scale = np.abs(r["forces"]).max()
-    assert de < 1e-3, de
+    # atomic energies reach 1e4 kcal/mol in so dense a cluster: float32 rounding, relative
+    e_atom = abs(r["energy"][0]) * HARTREE_TO_KCALMOL / 120
+    assert de < 2e-6 * e_atom + 1e-4, (de, e_atom)
     np.testing.assert_allclose(f.cpu().numpy(), r["forces"], rtol=0, atol=1e-4 * scale)
