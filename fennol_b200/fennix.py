@@ -38,6 +38,7 @@ from __future__ import annotations
 
 import dataclasses
 import re
+import weakref
 from collections import OrderedDict
 from copy import deepcopy
 from typing import Any, ClassVar, Dict, Optional, Sequence, Tuple
@@ -441,16 +442,13 @@ class SpeciesIndexer:
     def __call__(self, state, inputs, return_state_update=False, add_margin=False):
         species = np.asarray(inputs["species"], dtype=np.int32)
         nat = species.shape[0]
-        present, counts = np.unique(species, return_counts=True)
+        members = _species_members(inputs, species)
         new_state, state_up = dict(state), {}
         sizes = dict(state.get("sizes", {}))
         new_sizes = dict(sizes)
         grew = False
-        counts_of = {}
-        for s, c in zip(present.tolist(), counts.tolist()):
-            if s <= 0:
-                continue
-            counts_of[s] = c
+        counts_of = {s: len(m) for s, m in members.items()}
+        for s, c in counts_of.items():
             if c > sizes.get(s, 0):
                 grew = True
                 extra = state.get("add_atoms", self.add_atoms)
@@ -471,21 +469,18 @@ class SpeciesIndexer:
             for i, el in enumerate(order):
                 z = PERIODIC_TABLE_REV_IDX[el]
                 if z in counts_of:
-                    index[i, :counts_of[z]] = np.nonzero(species == z)[0]
+                    index[i, :counts_of[z]] = members[z]
         else:
             index = {PERIODIC_TABLE[s]: np.full(c, nat, dtype=np.int32) for s, c in new_sizes.items()}
             for s, c in counts_of.items():
-                index[PERIODIC_TABLE[s]][:c] = np.nonzero(species == s)[0]
+                index[PERIODIC_TABLE[s]][:c] = members[s]
         output = {**inputs, self.output_key: index, self.output_key + "_overflow": False}
         return (new_state, output, state_up) if return_state_update else (new_state, output)
 
     def process(self, state, inputs):
         species = np.asarray(inputs["species"], dtype=np.int32)
         sizes = state.get("sizes", {})
-        overflow = False
-        for s, c in zip(*np.unique(species, return_counts=True)):
-            if s > 0 and c > sizes.get(int(s), 0):
-                overflow = True
+        overflow = any(len(m) > sizes.get(s, 0) for s, m in _species_members(inputs, species).items())
         _, out = self(state, inputs)
         out[self.output_key + "_overflow"] = overflow
         return out
@@ -496,6 +491,27 @@ class SpeciesIndexer:
     def check_reallocate(self, state, inputs, parent_overflow=False):
         return _check_reallocate(self, state, inputs, parent_overflow,
                                  inputs[self.output_key + "_overflow"])
+
+
+_MEMBERS: "weakref.WeakKeyDictionary[BatchLayout, Dict[int, np.ndarray]]" = weakref.WeakKeyDictionary()
+
+
+def _species_members(inputs, species: np.ndarray) -> Dict[int, np.ndarray]:
+    """Atom indices of each atomic number (> 0) present, ascending; kept with
+    the batch layout, which changes whenever the species do."""
+    layout = inputs.get("_layout")
+    hit = _MEMBERS.get(layout) if layout is not None else None
+    if hit is not None:
+        return hit
+    order = np.argsort(species, kind="stable").astype(np.int32)
+    z, first = np.unique(species[order], return_index=True)
+    bounds = list(first) + [len(order)]
+    members = {int(v): order[bounds[k]:bounds[k + 1]] for k, v in enumerate(z) if v > 0}
+    for m in members.values():
+        m.flags.writeable = False
+    if layout is not None:
+        _MEMBERS[layout] = members
+    return members
 
 
 def _check_reallocate(layer, state, inputs, parent_overflow, own_overflow):
@@ -561,13 +577,6 @@ class PreprocessingChain:
         species = np.asarray(_host(inputs["species"]), dtype=np.int32).reshape(-1)
         nat = species.shape[0]
         natoms = np.asarray(_host(inputs.get("natoms", [nat])), dtype=np.int32).reshape(-1)
-        if int(natoms.sum()) != nat:
-            raise ValueError("natoms does not add up to the number of atoms")
-        batch_index = inputs.get("batch_index")
-        expected = np.repeat(np.arange(natoms.shape[0], dtype=np.int32), natoms)
-        if batch_index is not None and not np.array_equal(np.asarray(_host(batch_index)), expected):
-            raise ValueError("atoms must be grouped by system in batch order")
-        out = {**inputs, "species": species, "natoms": natoms, "batch_index": expected}
         cells = recips = None
         if "cells" in inputs:
             given = np.asarray(_host(inputs["cells"]))
@@ -582,19 +591,35 @@ class PreprocessingChain:
                 recips = np.linalg.inv(given)
             recips = recips.astype(np.float32)
             cells = given.astype(np.float32)
-            out["cells"] = cells
-            out["reciprocal_cells"] = recips
         minimum_image = "minimum_image" in inputs.get("flags", {})
-        if self.species_order:
-            sidx = AEVConfig(species_order=self.species_order).species_index(species)
-        else:
-            sidx = np.zeros(nat, np.int32)
-        key = (species.tobytes(), natoms.tobytes(), None if cells is None else cells.tobytes(),
-               None if recips is None else recips.tobytes(), minimum_image)
-        if key != self._layout_key:
+        # the layout (species-sorted rows, cell plans) is rebuilt only when the
+        # species, system sizes, cells or image convention change; a repeated
+        # system costs one comparison per array
+        c = self._layout_key
+        if not (c is not None and c[4] == minimum_image and _same(c[0], species)
+                and _same(c[1], natoms) and _same(c[2], cells) and _same(c[3], recips)):
+            if int(natoms.sum()) != nat:
+                raise ValueError("natoms does not add up to the number of atoms")
+            if self.species_order:
+                sidx = AEVConfig(species_order=self.species_order).species_index(species)
+            else:
+                sidx = np.zeros(nat, np.int32)
             cl = None if cells is None else list(cells)
             self._layout = BatchLayout(sidx, natoms, cl, minimum_image, self.device, reciprocal_cells=recips)
-            self._layout_key = key
+            expected = np.repeat(np.arange(natoms.shape[0], dtype=np.int32), natoms)
+            frozen = [None if a is None else a.copy() for a in (species, natoms, cells, recips)]
+            for a in frozen + [expected]:
+                if a is not None:
+                    a.flags.writeable = False
+            c = self._layout_key = (*frozen, minimum_image, expected)
+        expected = c[5]
+        batch_index = inputs.get("batch_index")
+        if batch_index is not None and not np.array_equal(np.asarray(_host(batch_index)), expected):
+            raise ValueError("atoms must be grouped by system in batch order")
+        out = {**inputs, "species": c[0], "natoms": c[1], "batch_index": expected}
+        if cells is not None:
+            out["cells"] = c[2]
+            out["reciprocal_cells"] = c[3]
         coords = torch.as_tensor(inputs["coordinates"], dtype=torch.float32)
         coords = coords.to(self.device, non_blocking=True).reshape(-1, 3).contiguous()
         out["_layout"] = self._layout
@@ -646,6 +671,18 @@ class PreprocessingChain:
                 for k, v in layer.get_graph_properties().items():
                     props[k] = {**props.get(k, {}), **v}
         return props
+
+
+def _scaled(x: torch.Tensor, fac: float) -> torch.Tensor:
+    """``x * fac`` as a new tensor; ``x`` itself (already a copy owned by the
+    caller) when the factor is 1."""
+    return x if fac == 1.0 else x * fac
+
+
+def _same(a, b) -> bool:
+    if a is None or b is None:
+        return a is b
+    return a.shape == b.shape and np.array_equal(a, b)
 
 
 def _host(x):
@@ -909,8 +946,48 @@ class FENNIX:
         self.preproc_state = state
         return out
 
+    def _prepare(self, gpu_preprocessing: bool, inputs):
+        """Preprocessing for one evaluation.  Once the chain has sized its
+        capacities, its layers run at those capacities (``process``) and the
+        graph layers' overflow words are read together with the evaluation's
+        own status, one host synchronisation per call.  Returns the processed
+        inputs and the device status words still to check (None when the
+        capacities were checked already)."""
+        if not self._sized:
+            return self.preprocess(use_gpu=gpu_preprocessing, **inputs), None
+        chain = self.preprocessing
+        out = chain.process(self.preproc_state, chain.check_input(inputs))
+        pending, seen = [], set()
+        for key, val in out.items():
+            if key.endswith("_overflow") and val is True:
+                return self.preprocess(use_gpu=gpu_preprocessing, **inputs), None
+            st = val.get("status") if isinstance(val, dict) else None
+            if isinstance(st, torch.Tensor) and id(st) not in seen:
+                seen.add(id(st))
+                pending.append(st)
+        return out, pending
+
+    def _status_host(self, rows: int) -> torch.Tensor:
+        buf = getattr(self, "_status_pinned", None)
+        if buf is None or buf.shape[0] < rows:
+            buf = torch.zeros((max(rows, 4), _lib.STATUS_WORDS), dtype=torch.int32).pin_memory()
+            self._status_pinned = buf
+        return buf
+
+    def _run(self, variables, gpu_preprocessing: bool, inputs, **want):
+        """Preprocess and evaluate; a capacity that overflowed at the sized
+        capacities reruns the call through the growing preprocessing path."""
+        if variables is None:
+            variables = self.variables
+        prepared, pending = self._prepare(gpu_preprocessing, inputs)
+        out = self._evaluate(variables, prepared, pending=pending, **want)
+        if out is None:
+            prepared = self.preprocess(use_gpu=gpu_preprocessing, **inputs)
+            out = self._evaluate(variables, prepared, **want)
+        return out
+
     def _evaluate(self, variables, inputs, want_forces: bool, want_embedding: bool = False,
-                  want_virial: bool = False):
+                  want_virial: bool = False, pending=None):
         pot = self._potential(variables)
         layout: BatchLayout = inputs["_layout"]
         ws = self._workspace(pot, layout)
@@ -921,10 +998,26 @@ class FENNIX:
              ws.xyzs.data_ptr(), st)
         view = _RowsView(rows)
         pot.launch_forces(layout, view, ws, st, want_forces, want_virial)
-        status = ws.status.cpu().numpy()
-        if pot.precision != _lib.MLP_FP32 and int(ws.mlp_ws[:4].view(torch.int32)[0]):
+        # every status word of the call in one read: the evaluation's, the
+        # MLP kernel's error word and the graph layers' overflow words
+        words = [ws.status] + list(pending or ())
+        host = self._status_host(len(words) + 1)
+        for k, w in enumerate(words):
+            host[k].copy_(w, non_blocking=True)
+        mlp_err = host[len(words), :1]
+        if pot.precision != _lib.MLP_FP32:
+            mlp_err.copy_(ws.mlp_ws[:4].view(torch.int32), non_blocking=True)
+        else:
+            mlp_err.zero_()
+        torch.cuda.current_stream(self.device).synchronize()
+        host_words = host[:len(words) + 1].numpy().copy()
+        status, graph_words = host_words[0], host_words[1:len(words)]
+        if int(host_words[len(words), 0]):
             ws.mlp_ws[:4].view(torch.int32).zero_()
             raise _lib.KernelTimeout("species MLP: a bounded wait inside the tensor-core kernel ran out")
+        if graph_words.size and (graph_words[:, _lib.ST_NBR_OVERFLOW].any()
+                                 or graph_words[:, _lib.ST_FILTER_OVERFLOW].any()):
+            return None
         if status[_lib.ST_NONFINITE]:
             raise _lib.NonFiniteError("non-finite positions, energies or forces")
         if status[_lib.ST_ANG_OVERFLOW]:
@@ -954,40 +1047,27 @@ class FENNIX:
     def __call__(self, variables=None, gpu_preprocessing: bool = False, **inputs) -> Dict[str, Any]:
         """Preprocess and apply the modules; the output holds the embedding
         (float32, [N, F] in atom order), atomic energies and total energy."""
-        if variables is None:
-            variables = self.variables
-        inputs = self.preprocess(use_gpu=gpu_preprocessing, **inputs)
-        return self._evaluate(variables, inputs, want_forces=False, want_embedding=True)
+        return self._run(variables, gpu_preprocessing, inputs, want_forces=False, want_embedding=True)
 
     def total_energy(self, variables=None, unit=None, gpu_preprocessing: bool = False, **inputs):
-        if variables is None:
-            variables = self.variables
-        inputs = self.preprocess(use_gpu=gpu_preprocessing, **inputs)
-        out = self._evaluate(variables, inputs, want_forces=False)
-        e = out["total_energy"] * self._unit_factor(unit)
-        return e, out
+        out = self._run(variables, gpu_preprocessing, inputs, want_forces=False)
+        return _scaled(out["total_energy"], self._unit_factor(unit)), out
 
     def energy_and_forces(self, variables=None, unit=None, gpu_preprocessing: bool = False, **inputs):
         """Total energies [B] (float64) and forces [N, 3] (float32) in the
         model's energy unit (per Angstrom), or in ``unit``."""
-        if variables is None:
-            variables = self.variables
-        inputs = self.preprocess(use_gpu=gpu_preprocessing, **inputs)
-        out = self._evaluate(variables, inputs, want_forces=True)
+        out = self._run(variables, gpu_preprocessing, inputs, want_forces=True)
         fac = self._unit_factor(unit)
-        e, f = out["total_energy"] * fac, out["forces"] * fac
-        return e, f, out
+        return _scaled(out["total_energy"], fac), _scaled(out["forces"], fac), out
 
     def energy_and_forces_and_virial(self, variables=None, unit=None, gpu_preprocessing: bool = False,
                                      **inputs):
         """Energies, forces and ``virial_tensor`` [B, 3, 3] = dE/dS of the
         deformation x -> x S, cell -> cell S at S = 1 (``fennix.py:320-347``)."""
-        if variables is None:
-            variables = self.variables
-        inputs = self.preprocess(use_gpu=gpu_preprocessing, **inputs)
-        out = self._evaluate(variables, inputs, want_forces=True, want_virial=True)
+        out = self._run(variables, gpu_preprocessing, inputs, want_forces=True, want_virial=True)
         fac = self._unit_factor(unit)
-        return out["total_energy"] * fac, out["forces"] * fac, out["virial_tensor"] * fac, out
+        return (_scaled(out["total_energy"], fac), _scaled(out["forces"], fac),
+                _scaled(out["virial_tensor"], fac), out)
 
     def set_energy_terms(self, energy_terms, jit: bool = True) -> None:
         """Select the energy terms of ``total_energy`` (``fennix.py:180-270``):

@@ -94,6 +94,33 @@ def test_gpu_preprocessing_reallocates(cuda_device):
     np.testing.assert_allclose(f1.cpu().numpy(), f0.cpu().numpy(), rtol=0, atol=1e-7)
 
 
+def test_sized_call_regrows_on_denser_input(cuda_device):
+    """A sized model launches its graph layers at the stored capacities and
+    checks their overflow words with the evaluation's status; a denser input
+    overflows them, and the call reruns through the growing path."""
+    s = water_box(8, seed=11)
+    m = make_model()
+    args = dict(species=s.species, natoms=np.array([s.natoms]), flags={"minimum_image": True})
+    e0, f0, _ = m.energy_and_forces(coordinates=s.coordinates, cells=s.cell[None], **args)
+    e0b, f0b, _ = m.energy_and_forces(coordinates=s.coordinates, cells=s.cell[None], **args)
+    # the force adjoint accumulates with float32 atomics: the order of the
+    # additions, and so the last bits, can differ between two evaluations
+    assert float(e0b[0]) == float(e0[0])
+    np.testing.assert_allclose(f0b.cpu().numpy(), f0.cpu().numpy(), rtol=0, atol=1e-6)
+    caps = [dict(x) for x in m.preproc_state["layers_state"]]
+    squeeze = 0.82
+    dense = dict(coordinates=(s.coordinates * squeeze).astype(np.float32),
+                 cells=(s.cell * squeeze)[None], **args)
+    e1, f1, _ = m.energy_and_forces(**dense)
+    grown = m.preproc_state["layers_state"]
+    assert grown[0]["max_neigh"] > caps[0]["max_neigh"]
+    assert grown[1]["max_neigh"] >= caps[1]["max_neigh"]
+    fresh = make_model()
+    e2, f2, _ = fresh.energy_and_forces(**dense)
+    np.testing.assert_allclose(e1.cpu().numpy(), e2.cpu().numpy(), rtol=0, atol=1e-9)
+    np.testing.assert_allclose(f1.cpu().numpy(), f2.cpu().numpy(), rtol=0, atol=1e-6)
+
+
 def test_skin_update_matches_fresh_build(cuda_device):
     s = water_box(8, seed=7)
     m = make_model()
