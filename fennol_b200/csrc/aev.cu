@@ -662,30 +662,47 @@ k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ a
   int* blk_p = blk_o + kMaxBlk;                          // species-pair index
   float* blk_r1 = reinterpret_cast<float*>(blk_p + kMaxBlk);  // 1 / n1
   float* blk_r2 = blk_r1 + kMaxBlk;                           // 1 / n2
-  if (lane == 0) {
+  // Lane l of round q takes the species pair (s1, s2) = divmod(32 q + l, S),
+  // kept when s1 <= s2: lane order is the s1-major order of the blocks.  A
+  // ballot numbers the non-empty blocks and a warp scan accumulates their
+  // first triplets.
+  {
     int nb = 0, tot = 0;
-    for (int s1 = 0; s1 < S; ++s1) {
-      const int n1 = min(st.cntw[S + s1], st.capa);
-      const int o1 = st.cntw[3 * S + s1] - st.cntw[S + s1];  // running offset ended at off + count
-      if (n1 == 0) continue;
-      for (int s2 = s1; s2 < S; ++s2) {
-        const int n2 = min(st.cntw[S + s2], st.capa);
-        const int o2 = st.cntw[3 * S + s2] - st.cntw[S + s2];
-        int T = s1 == s2 ? n1 * (n1 - 1) / 2 : n1 * n2;
+    for (int l0 = 0; l0 < S * S; l0 += 32) {
+      const int l = l0 + lane;
+      const int s1 = l / S, s2 = l - (l / S) * S;
+      int T = 0, n1 = 0, n2 = 0, o1 = 0, o2 = 0;
+      if (l < S * S && s1 <= s2) {
+        n1 = min(st.cntw[S + s1], st.capa);
+        n2 = min(st.cntw[S + s2], st.capa);
+        o1 = st.cntw[3 * S + s1] - st.cntw[S + s1];  // running offset ended at off + count
+        o2 = st.cntw[3 * S + s2] - st.cntw[S + s2];
+        T = s1 == s2 ? n1 * (n1 - 1) / 2 : n1 * n2;
         if (o1 + n1 > st.capa || o2 + n2 > st.capa) T = 0;
-        if (T == 0) continue;
-        blk_cum[nb] = tot;
-        blk_n[nb] = n1 | (n2 << 12) | ((s1 == s2) << 24);
-        blk_o[nb] = o1 | (o2 << 12);
-        blk_p[nb] = triu_pair(s1, s2, S);
-        blk_r1[nb] = 1.0f / (float)n1;
-        blk_r2[nb] = 1.0f / (float)n2;
-        tot += T;
-        ++nb;
       }
+      const unsigned has = __ballot_sync(0xffffffffu, T > 0);
+      int incl = T;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      if (T > 0) {
+        const int k = nb + __popc(has & ((1u << lane) - 1u));
+        blk_cum[k] = tot + incl - T;
+        blk_n[k] = n1 | (n2 << 12) | ((s1 == s2) << 24);
+        blk_o[k] = o1 | (o2 << 12);
+        blk_p[k] = triu_pair(s1, s2, S);
+        blk_r1[k] = 1.0f / (float)n1;
+        blk_r2[k] = 1.0f / (float)n2;
+      }
+      nb += __popc(has);
+      tot += __shfl_sync(0xffffffffu, incl, 31);
     }
-    blk_cum[nb] = tot;
-    blk_cum[kMaxBlk + 1] = nb;
+    if (lane == 0) {
+      blk_cum[nb] = tot;
+      blk_cum[kMaxBlk + 1] = nb;
+    }
   }
   __syncwarp();
   const int nblk = blk_cum[kMaxBlk + 1];
