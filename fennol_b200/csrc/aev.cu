@@ -418,36 +418,48 @@ __device__ __forceinline__ void store_feature(int out_kind, void* out, void* out
   }
 }
 
-// Warp-collective copy of one centre's staged neighbourhood into the shared
-// Stage view `dst` (carved at dst_base) from a global record of the same
-// layout (carve_stage(.., cap, false)) at src_base: the cnt unsorted edges
-// (vector, d^2, key), the na angular entries (unit vector and d, fc and dfc,
-// row slot) and the 4 S counters.  The forward saves the record for the
-// adjoint of the same step, which then skips the gathers and the sort.
-// Every global address is formed from src_base plus the array's offset in
-// the layout (a difference of two shared pointers): a pointer computed from
-// a shared one would be taken as a shared-window address.
+// Asynchronous global -> shared copy of B = 4, 8 or 16 bytes (both addresses
+// B-aligned); a thread's copies have landed after cp_async_wait_all.
+template <int B>
+__device__ __forceinline__ void cp_async(void* smem_dst, const void* gmem_src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(gmem_src), "n"(B) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Global address of the array that `p` points to in a shared Stage carved at
+// dst_base, inside a global record of the same layout at src_base.  Every
+// global address is formed from src_base plus the array's offset in the
+// layout (a difference of two shared pointers): a pointer computed from a
+// shared one would be taken as a shared-window address.
 template <typename T>
 __device__ __forceinline__ const T* in_record(const char* src_base, const char* dst_base, const T* p) {
   return reinterpret_cast<const T*>(src_base + (reinterpret_cast<const char*>(p) - dst_base));
 }
-__device__ __forceinline__ void copy_stage(const Stage& dst, const char* dst_base, const char* src_base, int cnt,
-                                           int na, int S, int lane) {
+
+// Warp-collective, asynchronous copy of one centre's staged neighbourhood
+// into the shared Stage view `dst` (carved at dst_base) from a global record
+// of the same layout (carve_stage(.., cap, false)) at src_base: the cnt
+// unsorted edges (vector, d^2, key) and the na angular entries (unit vector
+// and d, fc and dfc, row slot).  The forward saves the record for the adjoint
+// of the same step, which then skips the gathers and the sort.  Every copy is
+// in flight at once; the caller waits (cp_async_wait_all, then __syncwarp).
+__device__ __forceinline__ void copy_stage_async(const Stage& dst, const char* dst_base, const char* src_base,
+                                                 int cnt, int na, int lane) {
   const float4* tmp = in_record(src_base, dst_base, dst.tmp);
   const int* tkey = in_record(src_base, dst_base, dst.tkey);
   for (int k = lane; k < cnt; k += 32) {
-    dst.tmp[k] = tmp[k];
-    dst.tkey[k] = tkey[k];
+    cp_async<16>(dst.tmp + k, tmp + k);
+    cp_async<4>(dst.tkey + k, tkey + k);
   }
   const float4* au = in_record(src_base, dst_base, dst.au);
   const float2* af = in_record(src_base, dst_base, dst.af);
   const int* aslot = in_record(src_base, dst_base, dst.aslot);
   for (int k = lane; k < na; k += 32) {
-    dst.au[k] = au[k];
-    dst.af[k] = af[k];
-    dst.aslot[k] = aslot[k];
+    cp_async<16>(dst.au + k, au + k);
+    cp_async<8>(dst.af + k, af + k);
+    cp_async<4>(dst.aslot + k, aslot + k);
   }
-  if (lane < 4 * S) dst.cntw[lane] = in_record(src_base, dst_base, dst.cntw)[lane];
 }
 
 template <int RD, int AD, int AS, int ZN>
@@ -600,28 +612,41 @@ k_aev_backward(const float4* __restrict__ xyzs, int n, const int* __restrict__ a
   float* gr = (float*)(base + stage_bytes(cap, false));               // [S][RD+1]
   int* blkw = (int*)(gr + S * (RD + 1));                              // block table
 
-  const float* g = daev + (size_t)atom_row[i] * ld;
+  // Two dependent rounds of global loads: the row index, row length and
+  // (staged) the per-species counters, then every copy of the dE/dAEV row and
+  // of the staged record at once, as asynchronous copies into shared memory.
+  const int arow = atom_row[i];
+  int cnt = nbr_count[i];
+  const char* rec = nullptr;
+  int cw = 0;
+  if constexpr (kStaged) {
+    // the forward of this step staged this centre already
+    rec = stage_g + (size_t)i * stage_bytes(cap, false);
+    if (lane < 4 * S) cw = in_record(rec, base, st.cntw)[lane];
+  }
+  const float* g = daev + (size_t)arow * ld;
   const int FR = S * RD;
-  for (int col = lane; col < FR; col += 32) gr[(col / RD) * (RD + 1) + col % RD] = g[col];
+  for (int col = lane; col < FR; col += 32) cp_async<4>(gr + (col / RD) * (RD + 1) + col % RD, g + col);
   const float4 pi = xyzs[i];
   float c[9];
   load_cell(sys_cell, atom_sys[i], c);
-  int cnt = nbr_count[i];
   if (cnt > cap) cnt = cap;
   const size_t row = (size_t)i * cap;
   if constexpr (kStaged) {
-    // the forward of this step staged this centre already
-    const char* rec = stage_g + (size_t)i * stage_bytes(cap, false);
-    const int* cw = in_record(rec, base, st.cntw);
-    int na = 0;
-    for (int s2 = 0; s2 < S; ++s2) na += cw[S + s2];
-    copy_stage(st, base, rec, cnt, min(na, st.capa), S, lane);
+    if (lane < 4 * S) st.cntw[lane] = cw;
+    int na = lane >= S && lane < 2 * S ? cw : 0;  // angular counts per species
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) na += __shfl_xor_sync(0xffffffffu, na, o);
+    copy_stage_async(st, base, rec, cnt, min(na, st.capa), lane);
+    cp_async_wait_all();
     __syncwarp();
   } else {
     int cnt_r, off_r, cnt_a, off_a, na;
     stage_row<true, false, false>(st, st.cntw, xyzs, pi, c, nbr_j, nbr_shift, row, cnt, K, lane, cnt_r, off_r,
                                   cnt_a, off_a, na);
     if (na > st.capa && lane == 0) status_set(status, ST_ANG_OVERFLOW);
+    cp_async_wait_all();
+    __syncwarp();
   }
 
   // ---- radial: lane per neighbour (row order), gradient into gk[4k..4k+2]
