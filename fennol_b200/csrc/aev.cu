@@ -266,23 +266,25 @@ __device__ __forceinline__ void stage_row(const Stage& st, int* cntw, const floa
   const int S = K.S;
   // cntw[0..S): radial counts, [S..2S): angular counts, [2S..4S): running offsets
   if (lane < 4 * S) cntw[lane] = 0;
+  // gather: the edge geometry of every row entry.  No warp-collective step
+  // here, so the loads of consecutive rounds are in flight together.
+#pragma unroll 2
+  for (int k = lane; k < cnt; k += 32) {
+    const int j = __ldg(nbr_j + row + k);
+    const unsigned sh = __ldg(nbr_shift + row + k);
+    const float4 pj = xyzs[j];
+    float vx, vy, vz;
+    edge_vec(pi, pj, sh, c, vx, vy, vz);
+    const float d2 = dist2_exact(vx, vy, vz);
+    st.tmp[k] = make_float4(vx, vy, vz, d2);
+    st.tkey[k] = __float_as_int(pj.w) | ((d2 < K.rca2) << 8);
+  }
   __syncwarp();
   const unsigned lt = (1u << lane) - 1u;
+  // count the entries per species (radial) and per species within rca (angular)
   for (int k0 = 0; k0 < cnt; k0 += 32) {
     const int k = k0 + lane;
-    int key = -1;
-    if (k < cnt) {
-      int j = __ldg(nbr_j + row + k);
-      unsigned sh = __ldg(nbr_shift + row + k);
-      float4 pj = xyzs[j];
-      float vx, vy, vz;
-      edge_vec(pi, pj, sh, c, vx, vy, vz);
-      float d2 = dist2_exact(vx, vy, vz);
-      int sj = __float_as_int(pj.w);
-      key = sj | ((d2 < K.rca2) << 8);
-      st.tmp[k] = make_float4(vx, vy, vz, d2);
-      st.tkey[k] = key;
-    }
+    const int key = k < cnt ? st.tkey[k] : -1;
     const unsigned grp = __match_any_sync(0xffffffffu, key);
     if (key >= 0 && (grp & lt) == 0) {  // group leader (two groups may share a species)
       const int sj = key & 0xFF;
