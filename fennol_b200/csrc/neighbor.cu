@@ -350,17 +350,113 @@ __device__ __forceinline__ void cell_row(int i, const int* __restrict__ atom_sys
   row_finish(i, count, cap, nbr_count, status, lane);
 }
 
+// ---------------------------------------------------------------------------
+// 4a'. cell-list rows with the stencil staged in shared memory: one block per
+//      cell gathers the candidates of its 27 stencil cells (position, index,
+//      wrap shift, stencil cell) once, and its warps build the rows of the
+//      cell's atoms from that copy; every candidate is read from global memory
+//      once per cell instead of once per atom.  Candidates are kept in the
+//      order of 4a (stencil cell, then atom index), so the rows are the same.
+//      A cell whose stencil holds more than kStageCand candidates falls back
+//      to the per-atom gathers of 4a.
+// ---------------------------------------------------------------------------
+constexpr int kStageCand = 1024;
+
 __global__ void __launch_bounds__(kBuildWarps * 32)
-k_build_cells(int n, const int* __restrict__ atom_sys, SysView sv, GraphWs w, float rc2, int cap,
-              int* __restrict__ nbr_j, unsigned* __restrict__ nbr_shift, int* __restrict__ nbr_count,
-              int* status, const int* enable_flag) {
+k_build_cells_staged(int ncells, const int* __restrict__ atom_sys, SysView sv, GraphWs w, float rc2, int cap,
+                     int* __restrict__ nbr_j, unsigned* __restrict__ nbr_shift, int* __restrict__ nbr_count,
+                     int* status, const int* enable_flag) {
   pdl_wait();
   if (enable_flag && *enable_flag == 0) return;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int i = blockIdx.x * kBuildWarps + warp; i < n; i += gridDim.x * kBuildWarps)
-    cell_row(i, atom_sys, sv, w, rc2, cap, nbr_j, nbr_shift, nbr_count, status, lane);
+  __shared__ float4 c_pos[kStageCand];
+  __shared__ int c_j[kStageCand];
+  __shared__ unsigned c_at[kStageCand];
+  __shared__ unsigned char c_sc[kStageCand];
+  __shared__ int s_first[28], s_start[27], s_wrap[27];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int cell = blockIdx.x; cell < ncells; cell += gridDim.x) {
+    const int a0 = w.starts[cell], na = w.starts[cell + 1] - a0;
+    if (na == 0) continue;  // block-uniform
+    const int b = atom_sys[w.cell_atoms[a0]];
+    const int mode = sv.mode[b];
+    const float* c = sv.cell + 9 * b;
+    const float* r = sv.recip + 9 * b;
+    const int* g = sv.grid + 4 * b;
+    const int nx = g[0], ny = g[1], nz = g[2], off = g[3];
+    const int local = cell - off;
+    const int cz = local % nz, cy = (local / nz) % ny, cx = local / (ny * nz);
+    if (warp == 0) {
+      int s0 = 0, cnt = 0, wrap = 0;
+      if (lane < 27) {
+        int ex = cx + lane / 9 - 1, ey = cy + (lane / 3) % 3 - 1, ez = cz + lane % 3 - 1;
+        int wx = 0, wy = 0, wz = 0;
+        if (ex < 0) { ex += nx; wx = -1; } else if (ex >= nx) { ex -= nx; wx = 1; }
+        if (ey < 0) { ey += ny; wy = -1; } else if (ey >= ny) { ey -= ny; wy = 1; }
+        if (ez < 0) { ez += nz; wz = -1; } else if (ez >= nz) { ez -= nz; wz = 1; }
+        const int nc = off + (ex * ny + ey) * nz + ez;
+        s0 = w.starts[nc];
+        cnt = w.starts[nc + 1] - s0;
+        wrap = (wx + 1) | ((wy + 1) << 2) | ((wz + 1) << 4);
+      }
+      int incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      if (lane < 27) {
+        s_first[lane] = incl - cnt;
+        s_start[lane] = s0;
+        s_wrap[lane] = wrap;
+      }
+      if (lane == 26) s_first[27] = incl;
+    }
+    __syncthreads();
+    const int total = s_first[27];
+    if (total <= kStageCand) {
+      for (int k = tid; k < total; k += kBuildWarps * 32) {
+        // stencil cell of candidate k: the last s < 27 with s_first[s] <= k
+        int sc = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1)
+          if (sc + step < 27 && s_first[sc + step] <= k) sc += step;
+        const int j = w.cell_atoms[s_start[sc] + k - s_first[sc]];
+        c_pos[k] = w.pos[j];
+        c_j[k] = j;
+        c_at[k] = w.at[j];
+        c_sc[k] = (unsigned char)sc;
+      }
+      __syncthreads();
+      for (int a = warp; a < na; a += kBuildWarps) {
+        const int i = w.cell_atoms[a0 + a];
+        const float4 pi = w.pos[i];
+        const unsigned ati = w.at[i];
+        const size_t base = (size_t)i * cap;
+        int count = 0;
+        for (int k0 = 0; k0 < total; k0 += 32) {
+          const int k = k0 + lane;
+          bool keep = false;
+          int j = -1;
+          unsigned sh = 0;
+          if (k < total) {
+            j = c_j[k];
+            if (j != i) {
+              const int swrap = s_wrap[c_sc[k]];
+              keep = pair_test(mode, pi, c_pos[k], ati, c_at[k], (swrap & 3) - 1, ((swrap >> 2) & 3) - 1,
+                               ((swrap >> 4) & 3) - 1, c, r, rc2, sh);
+            }
+          }
+          row_append(keep, j, sh, nbr_j, nbr_shift, base, cap, count, lane);
+        }
+        row_finish(i, count, cap, nbr_count, status, lane);
+      }
+    } else {
+      for (int a = warp; a < na; a += kBuildWarps)
+        cell_row(w.cell_atoms[a0 + a], atom_sys, sv, w, rc2, cap, nbr_j, nbr_shift, nbr_count, status, lane);
+    }
+    __syncthreads();  // the stencil tables and candidates are reused by the next cell
+  }
 }
-
 
 // ---------------------------------------------------------------------------
 // 4b. all-pairs rows (molecules, boxes too small for a 3x3x3 cell stencil).
@@ -573,8 +669,9 @@ extern "C" int fennol_graph_build(const float* coords, int natoms, const int* at
   // enable flag turns the build into a no-op
   int gw = std::min((natoms + kBuildWarps - 1) / kBuildWarps, 148 * 16);
   if (ncells_total > 0) {
-    FNL_LAUNCH_PDL(k_build_cells, gw, kBuildWarps * 32, 0, st, natoms, atom_sys, sv, w, rc2, capacity, nbr_j, nbr_shift,
-                                                    nbr_count, status, enable_flag);
+    const int gc = std::min(ncells_total, 148 * 16);
+    FNL_LAUNCH_PDL(k_build_cells_staged, gc, kBuildWarps * 32, 0, st, ncells_total, atom_sys, sv, w, rc2, capacity,
+                   nbr_j, nbr_shift, nbr_count, status, enable_flag);
     FNL_CHECK_LAUNCH();
   }
   FNL_LAUNCH_PDL(k_build_allpairs, gw, kBuildWarps * 32, 0, st, natoms, atom_sys, sv, w, rc2, capacity, nbr_j, nbr_shift,

@@ -921,6 +921,19 @@ class FENNIX:
             self._ws_cache = (layout, pot, Workspace(pot, layout))
         return self._ws_cache[2]
 
+    def _stage_buffer(self, n: int, cap: int) -> Optional[torch.Tensor]:
+        """Per-centre staging for the forward/adjoint pair of one call (the
+        forward saves each centre's sorted neighbourhood, the adjoint reads it
+        back instead of gathering and sorting again); kept across calls of the
+        same size, None above 4 GB."""
+        hit = getattr(self, "_stage_cache", None)
+        if hit is not None and hit[0] == (n, cap):
+            return hit[1]
+        nbytes = int(_lib.load().fennol_aev_stage_bytes(max(n, 1), cap))
+        buf = torch.empty(nbytes, dtype=torch.uint8, device=self.device) if nbytes <= (4 << 30) else None
+        self._stage_cache = ((n, cap), buf)
+        return buf
+
     def _unit_factor(self, unit) -> float:
         if unit is None:
             return 1.0
@@ -997,6 +1010,8 @@ class FENNIX:
         call("fennol_pack_atoms", inputs["_coords"].data_ptr(), layout.t_species.data_ptr(), layout.n,
              ws.xyzs.data_ptr(), st)
         view = _RowsView(rows)
+        if want_forces and not want_virial:
+            view.aev_stage = self._stage_buffer(layout.n, rows.capacity)
         pot.launch_forces(layout, view, ws, st, want_forces, want_virial)
         # every status word of the call in one read: the evaluation's, the
         # MLP kernel's error word and the graph layers' overflow words
