@@ -107,9 +107,11 @@ class NeighborRows:
 
     @classmethod
     def empty(cls, n: int, cap: int, cutoff: float, device) -> "NeighborRows":
+        # the builders write every row's count and its entries below it; the
+        # kernels and graph_edges read nothing past the count
         n = max(n, 1)
-        return cls(torch.zeros((n, cap), dtype=torch.int32, device=device),
-                   torch.zeros((n, cap), dtype=torch.int32, device=device),
+        return cls(torch.empty((n, cap), dtype=torch.int32, device=device),
+                   torch.empty((n, cap), dtype=torch.int32, device=device),
                    torch.zeros(n, dtype=torch.int32, device=device), float(cutoff))
 
 
@@ -251,7 +253,8 @@ class GraphGenerator:
         status = graph.get("status")
         if status is None:
             status = _status(layout.device)
-        status.zero_()
+        else:
+            status.zero_()
         rows = _build_rows(layout, coords, self.cutoff + skin, int(state["max_neigh"]), status)
         graph.update(status=status)
         if skin > 0:
@@ -355,7 +358,8 @@ class GraphFilter:
         status = graph.get("status")
         if status is None:
             status = _status(layout.device)
-        status.zero_()
+        else:
+            status.zero_()
         graph.update(cutoff=self.cutoff, parent_graph=self.parent_graph, status=status,
                      rows=_filter_rows(layout, coords, inputs[self.parent_graph]["rows"], self.cutoff,
                                        int(state["max_neigh"]), status),
@@ -1013,6 +1017,25 @@ class FENNIX:
         if want_forces and not want_virial:
             view.aev_stage = self._stage_buffer(layout.n, rows.capacity)
         pot.launch_forces(layout, view, ws, st, want_forces, want_virial)
+        # the outputs are enqueued before the status read, so that one host
+        # synchronisation covers them too
+        out = dict(inputs)
+        net_key = self.net_module.out_key
+        out[net_key] = ws.e_atom.clone()
+        if self.energy_terms is None:
+            out["total_energy"] = torch.zeros(layout.nsys, dtype=torch.float64, device=self.device)
+        else:
+            out["total_energy"] = ws.energy.clone()
+        if want_forces:
+            f = torch.empty((layout.n, 3), dtype=torch.float32, device=self.device)
+            call("fennol_forces_finalize", ws.forces4.data_ptr(), layout.n, 1.0, f.data_ptr(), st)
+            out["forces"] = f if self.energy_terms is not None else torch.zeros_like(f)
+        if want_virial:
+            vir = ws.virial.clone()
+            out["virial_tensor"] = vir if self.energy_terms is not None else torch.zeros_like(vir)
+        if want_embedding:
+            out[self.aev_module.embedding_key] = _embedding_from_rows(ws, layout,
+                                                                       self.aev_config.aev_length)
         # every status word of the call in one read: the evaluation's, the
         # MLP kernel's error word and the graph layers' overflow words
         words = [ws.status] + list(pending or ())
@@ -1038,23 +1061,6 @@ class FENNIX:
         if status[_lib.ST_ANG_OVERFLOW]:
             raise RuntimeError(f"more than {_lib.MAX_ANGULAR_NEIGHBORS} angular neighbours "
                                f"({int(status[_lib.ST_ANG_MAXCOUNT])}) around one atom")
-        out = dict(inputs)
-        net_key = self.net_module.out_key
-        out[net_key] = ws.e_atom.clone()
-        if self.energy_terms is None:
-            out["total_energy"] = torch.zeros(layout.nsys, dtype=torch.float64, device=self.device)
-        else:
-            out["total_energy"] = ws.energy.clone()
-        if want_forces:
-            call("fennol_forces_finalize", ws.forces4.data_ptr(), layout.n, 1.0, ws.forces.data_ptr(), st)
-            f = ws.forces.clone()
-            out["forces"] = f if self.energy_terms is not None else torch.zeros_like(f)
-        if want_virial:
-            vir = ws.virial.clone()
-            out["virial_tensor"] = vir if self.energy_terms is not None else torch.zeros_like(vir)
-        if want_embedding:
-            out[self.aev_module.embedding_key] = _embedding_from_rows(ws, layout,
-                                                                       self.aev_config.aev_length)
         for k in ("_layout", "_coords"):
             out.pop(k, None)
         return out

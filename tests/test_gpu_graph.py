@@ -59,6 +59,22 @@ def test_water_box_pairs_cell_list(pot, n_side, seed, mi):
         assert _same(canon, ref), (n_side, rc, len(canon["p1"]), len(ref["p1"]))
 
 
+def test_crowded_stencil_fallback_pairs(pot):
+    """A box whose stencils partly hold more candidates than a block stages
+    (a dense 4 A clump of 700 extra atoms): those cells take the per-atom
+    gather path, the others the staged one; the pair set stays the oracle's."""
+    s = water_box(8, seed=4)
+    rng = np.random.default_rng(4)
+    corner = s.coordinates.min(0) + 3.0
+    clump = (corner + rng.uniform(0.0, 4.0, (700, 3))).astype(np.float32)
+    xyz = np.concatenate([s.coordinates, clump]).astype(np.float32)
+    sp = np.concatenate([s.species, np.full(700, 1, s.species.dtype)])
+    for mi in (True, False):
+        ref = graph_fp32.pair_list(xyz, [len(sp)], s.cell[None], None, 5.2, mi)
+        canon, sym, *_ = _gpu_pairs(pot, xyz, sp, [len(sp)], s.cell[None], 5.2, mi)
+        assert sym and _same(canon, ref), (mi, len(canon["p1"]), len(ref["p1"]))
+
+
 def test_molecule_batch_pairs(pot):
     mols = molecule_batch(20, seed=4)
     xyz = np.concatenate([m.coordinates for m in mols])
