@@ -125,6 +125,12 @@ __device__ __forceinline__ int run_at(unsigned long long mask, int c, int& len) 
   return s;
 }
 
+// Drop the 128-byte L2 line at a (128-byte aligned) without writing it back;
+// its contents become undefined.
+__device__ __forceinline__ void discard_l2(const void* a) {
+  asm volatile("discard.global.L2 [%0], 128;" ::"l"(a) : "memory");
+}
+
 __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
@@ -241,6 +247,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
     // ------------------------------------------------------------------ TMA producer
     // (with p.stall it issues nothing: the other roles' waits run out)
     if (lane == 0 && !p.stall) {
+      const uint64_t keep = l2_evict_last();
       uint32_t xq = 0, wq = 0;
       int item = 0;
       bool ok = true;
@@ -257,8 +264,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
             if (u > 0 && !(ok = wait_bar(&bars->x_empty[s], (u - 1) & 1, abort_flag, p.err, p.timeout_ns))) break;
             uint8_t* st = act + s * p.xstage;
             mbar_expect_tx(&bars->x_full[s], x_tx);
-            tma_load_2d(&maps.x, &bars->x_full[s], st, kc * BK, row0);
-            if (p.a_lo) tma_load_2d(&maps.xlo, &bars->x_full[s], st + kAtom, kc * BK, row0);
+            // the AEV tile is read once per model: kept in L2 ahead of other lines
+            tma_load_2d_hint(&maps.x, &bars->x_full[s], st, kc * BK, row0, keep);
+            if (p.a_lo) tma_load_2d_hint(&maps.xlo, &bars->x_full[s], st + kAtom, kc * BK, row0, keep);
             tma_load_2d(&maps.w1t, &bars->x_full[s], st + 2 * kAtom, kc * BK, g * p.d1);
             if (p.wf_lo) tma_load_2d(&maps.w1t_lo, &bars->x_full[s], st + 4 * kAtom, kc * BK, g * p.d1);
           }
@@ -443,6 +451,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
     bool ok = true;
     // per-CTA CELU' scratch, column-major [d1 + d2][128] so that a warp's 32 rows are contiguous
     float* dc = p.dc + (size_t)blockIdx.x * BM * (p.d1 + p.d2) + r;
+    // this warp's 128-byte segment (32 rows) of CELU' column 0
+    float* dc_lines = p.dc + (size_t)blockIdx.x * BM * (p.d1 + p.d2) + 32 * q;
     const float inv_alpha = 1.0f / p.alpha;
     const bool with_lo = p.a_lo != 0;    // forward activations
     const bool grad_lo = p.g_lo != 0;    // input-gradient operands
@@ -503,6 +513,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
         tmem_ld32(tmem + b * 256 + lane_base + cc * 32, v);
 #pragma unroll
         for (int k = 0; k < 32; ++k) v[k] = (v[k] * inv_s) * dd[k];
+        // the warp has read these 32 columns of its 32 rows for the last time:
+        // their L2 lines are dropped without a write-back (the next item
+        // rewrites them before reading)
+        __syncwarp();
+        discard_l2(dc_lines + (size_t)(dc0 + cc * 32 + lane) * BM);
         act_store<F16>(act, r, cc * 32, v, grad_lo);
         publish_atom(cc >> 1);
       }
@@ -628,10 +643,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
             fence_proxy_async();
             __syncwarp();
             if (lane == 0) {
+              // the dE/dAEV block is added to once per model: kept in L2
               if (m == 0)
-                tma_store_2d(&maps.dx, tile, c0 * 64 + cc * 32, dx_row);
+                tma_store_2d_hint(&maps.dx, tile, c0 * 64 + cc * 32, dx_row, l2_evict_last());
               else
-                tma_add_2d(&maps.dx, tile, c0 * 64 + cc * 32, dx_row);
+                tma_add_2d_hint(&maps.dx, tile, c0 * 64 + cc * 32, dx_row, l2_evict_last());
               bulk_commit();
             }
           }
@@ -722,7 +738,7 @@ bool fnl_mlp_fused_supported(int precision, const fennol_mlp_weights* w) {
 }
 
 size_t fnl_mlp_fused_workspace(const fennol_mlp_weights* w) {
-  return 256 + (size_t)sm_count() * BM * (w->dims[1] + w->dims[2]) * sizeof(float);
+  return 256 + 128 + (size_t)sm_count() * BM * (w->dims[1] + w->dims[2]) * sizeof(float);
 }
 
 int fnl_mlp_fused(int precision, int rows, int ntiles, const int* tile_species, const int* tile_row,
@@ -796,7 +812,8 @@ int fnl_mlp_fused(int precision, int rows, int ntiles, const int* tile_species, 
     p.stall = 1;
     --g_stall_launches;
   }
-  p.dc = (float*)((char*)ws + 256);
+  // CELU' scratch on a 128-byte boundary: its L2 lines are discarded whole
+  p.dc = (float*)(((uintptr_t)ws + 256 + 127) & ~(uintptr_t)127);
   const size_t smem = kSmemMain + sizeof(Bars) + 1024;
   static bool attr[2] = {false, false};
   auto kern = f16 ? k_mlp_fused<true> : k_mlp_fused<false>;
