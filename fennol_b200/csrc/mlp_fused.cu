@@ -136,9 +136,11 @@ __device__ __forceinline__ void fence_proxy_async() {
 }
 // CELU and its derivative from one exponential: e = exp(z/alpha) for z <= 0,
 // celu = alpha (e - 1), celu' = e; both are z and 1 for z > 0.
-__device__ __forceinline__ void celu_pair(float z, float alpha, float inv_alpha, float& h, float& dh) {
-  const float e = __expf(fminf(z, 0.f) * inv_alpha);
-  h = z > 0.f ? z : alpha * (e - 1.f);
+__device__ __forceinline__ void celu_pair(float z, float alpha, float k2, float& h, float& dh) {
+  // k2 = log2(e) / alpha: e = 2^(min(z, 0) k2) by the SFU
+  float e;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(fminf(z, 0.f) * k2));
+  h = z > 0.f ? z : fmaf(alpha, e, -alpha);
   dh = z > 0.f ? 1.f : e;
 }
 
@@ -453,7 +455,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
     float* dc = p.dc + (size_t)blockIdx.x * BM * (p.d1 + p.d2) + r;
     // this warp's 128-byte segment (32 rows) of CELU' column 0
     float* dc_lines = p.dc + (size_t)blockIdx.x * BM * (p.d1 + p.d2) + 32 * q;
-    const float inv_alpha = 1.0f / p.alpha;
+    const float celu_k2 = 1.4426950408889634f / p.alpha;  // log2(e) / alpha
     const bool with_lo = p.a_lo != 0;    // forward activations
     const bool grad_lo = p.g_lo != 0;    // input-gradient operands
     auto take_acc = [&](uint32_t b) -> bool {
@@ -474,10 +476,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
       fence_proxy_async();
       mbar_arrive(&bars->act_ready[a]);
     };
-    // H = celu(Z / s_W + bias) -> act for columns [0, n); celu'(z) -> dc columns
-    // [dc0, dc0 + n).  The bias loads are issued before the TMEM load so that
-    // their latencies overlap.  inv_s = 1 / s_W (1 for the BF16 forms).
-    auto celu_layer = [&](uint32_t b, const float* bias, int n, int dc0, float inv_s) {
+    // H = celu(Z / s_W + bias) -> act for columns [0, n); celu'(z) / s_W' -> dc
+    // columns [dc0, dc0 + n), where s_W' is the scale of the weights the
+    // input gradient of this layer is taken through (a power of two, so the
+    // product is exact).  The bias loads are issued before the TMEM load so
+    // that their latencies overlap.  inv_s = 1 / s_W, dscale = 1 / s_W' (1 for
+    // the BF16 forms).
+    auto celu_layer = [&](uint32_t b, const float* bias, int n, int dc0, float inv_s, float dscale) {
       for (int cc = half; cc < n / 32; cc += 2) {
         float4 bb[8];
 #pragma unroll
@@ -492,18 +497,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
             float dh;
-            celu_pair(zz[u], p.alpha, inv_alpha, v[4 * k + u], dh);
-            dco[(size_t)(4 * k + u) * BM] = dh;  // column-major: the warp writes 128 contiguous bytes
+            celu_pair(zz[u], p.alpha, celu_k2, v[4 * k + u], dh);
+            dco[(size_t)(4 * k + u) * BM] = dh * dscale;  // column-major: the warp writes 128 contiguous bytes
           }
         }
         act_store<F16>(act, r, cc * 32, v, with_lo);
         publish_atom(cc >> 1);
       }
     };
-    // G = D / s_W * celu'(z) -> act for columns [0, n), celu' read back from dc
-    // columns [dc0, dc0 + n) (written by this thread); loads issued before the
-    // TMEM load.
-    auto mask_layer = [&](uint32_t b, int n, int dc0, float inv_s) {
+    // G = D / s_W * celu'(z) -> act for columns [0, n), celu'(z) / s_W read
+    // back from dc columns [dc0, dc0 + n) (written by this thread); loads
+    // issued before the TMEM load.
+    auto mask_layer = [&](uint32_t b, int n, int dc0) {
       for (int cc = half; cc < n / 32; cc += 2) {
         const float* dci = dc + (size_t)(dc0 + cc * 32) * BM;
         float dd[32];
@@ -512,7 +517,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
         float v[32];
         tmem_ld32(tmem + b * 256 + lane_base + cc * 32, v);
 #pragma unroll
-        for (int k = 0; k < 32; ++k) v[k] = (v[k] * inv_s) * dd[k];
+        for (int k = 0; k < 32; ++k) v[k] *= dd[k];
         // the warp has read these 32 columns of its 32 rows for the last time:
         // their L2 lines are dropped without a write-back (the next item
         // rewrites them before reading)
@@ -541,14 +546,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
         {
           const uint32_t b = job & 1;
           if (!(ok = take_acc(b))) break;
-          celu_layer(b, p.b1 + (size_t)g * p.d1, p.d1, 0, inv_s1);
+          celu_layer(b, p.b1 + (size_t)g * p.d1, p.d1, 0, inv_s1, inv_s2);
           release_acc(b);
         }
         // E2: H2 = celu(Z2 + b2) -> act; celu'(z2) -> dc[d1:d1+d2]
         {
           const uint32_t b = job & 1;
           if (!(ok = take_acc(b))) break;
-          celu_layer(b, p.b2 + (size_t)g * p.d2, p.d2, p.d1, inv_s2);
+          celu_layer(b, p.b2 + (size_t)g * p.d2, p.d2, p.d1, inv_s2, inv_s3);
           release_acc(b);
         }
         // E3: energy head; G3 = s_g w4 * celu'(z3) -> act.  Both column halves work;
@@ -577,7 +582,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
 #pragma unroll
               for (int u = 0; u < 4; ++u) {
                 float h, dh;
-                celu_pair(zz[u], p.alpha, inv_alpha, h, dh);
+                celu_pair(zz[u], p.alpha, celu_k2, h, dh);
                 e = fmaf(h, wv[u], e);
                 v[4 * k + u] = (s_g * wv[u]) * dh;
               }
@@ -604,14 +609,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fused(const __grid_constant
         {
           const uint32_t b = job & 1;
           if (!(ok = take_acc(b))) break;
-          mask_layer(b, p.d2, p.d1, inv_s3);
+          mask_layer(b, p.d2, p.d1);
           release_acc(b);
         }
         // E5: G1 = D1 * celu'(z1) -> act
         {
           const uint32_t b = job & 1;
           if (!(ok = take_acc(b))) break;
-          mask_layer(b, p.d1, 0, inv_s2);
+          mask_layer(b, p.d1, 0);
           release_acc(b);
         }
         // E6: dX chunks.  Each warp stages a 32 x 32 block (its 32 rows, 32
