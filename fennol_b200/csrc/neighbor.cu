@@ -361,19 +361,38 @@ __device__ __forceinline__ void cell_row(int i, const int* __restrict__ atom_sys
 //      to the per-atom gathers of 4a.
 // ---------------------------------------------------------------------------
 constexpr int kStageCand = 1024;
+constexpr int kCellWarps = 8;  // warps per cell block: the atoms of a cell (~14-24 in a liquid) are shared out
 
-__global__ void __launch_bounds__(kBuildWarps * 32)
+// Position moved into the box by whole cell vectors, -floor of its fractional
+// coordinates as the binning takes them (k_prepare).
+__device__ __forceinline__ float4 wrapped(float4 p, const float* c, const float* r) {
+  float x = p.x, y = p.y, z = p.z;
+  const float ax = -floorf(frac_exact(x, y, z, r, 0));
+  const float ay = -floorf(frac_exact(x, y, z, r, 1));
+  const float az = -floorf(frac_exact(x, y, z, r, 2));
+  add_shift(x, y, z, ax, ay, az, c);
+  return make_float4(x, y, z, 0.f);
+}
+
+__global__ void __launch_bounds__(kCellWarps * 32)
 k_build_cells_staged(int ncells, const int* __restrict__ atom_sys, SysView sv, GraphWs w, float rc2, int cap,
                      int* __restrict__ nbr_j, unsigned* __restrict__ nbr_shift, int* __restrict__ nbr_count,
                      int* status, const int* enable_flag) {
   pdl_wait();
   if (enable_flag && *enable_flag == 0) return;
   __shared__ float4 c_pos[kStageCand];
+  __shared__ float4 c_posw[kStageCand];  // minimum image: positions wrapped into the box (pre-test)
   __shared__ int c_j[kStageCand];
   __shared__ unsigned c_at[kStageCand];
   __shared__ unsigned char c_sc[kStageCand];
   __shared__ int s_first[28], s_start[27], s_wrap[27];
+  __shared__ float4 s_shift[27];               // wrap @ cell of each stencil cell
+  __shared__ int s_queue[kCellWarps][64];     // per warp: candidates that passed the pre-test
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  // pre-test threshold: a little above rc^2, far beyond the rounding difference
+  // between the pre-test's distance and the exact one
+  const float rc_pre = sqrtf(rc2) + 0.05f, rc2_pre = rc_pre * rc_pre;
   for (int cell = blockIdx.x; cell < ncells; cell += gridDim.x) {
     const int a0 = w.starts[cell], na = w.starts[cell + 1] - a0;
     if (na == 0) continue;  // block-uniform
@@ -408,50 +427,102 @@ k_build_cells_staged(int ncells, const int* __restrict__ atom_sys, SysView sv, G
         s_first[lane] = incl - cnt;
         s_start[lane] = s0;
         s_wrap[lane] = wrap;
+        const float wx = (float)((wrap & 3) - 1), wy = (float)(((wrap >> 2) & 3) - 1),
+                    wz = (float)(((wrap >> 4) & 3) - 1);
+        s_shift[lane] = make_float4(wx * c[0] + wy * c[3] + wz * c[6], wx * c[1] + wy * c[4] + wz * c[7],
+                                    wx * c[2] + wy * c[5] + wz * c[8], 0.f);
       }
       if (lane == 26) s_first[27] = incl;
     }
     __syncthreads();
     const int total = s_first[27];
     if (total <= kStageCand) {
-      for (int k = tid; k < total; k += kBuildWarps * 32) {
+      for (int k = tid; k < total; k += kCellWarps * 32) {
         // stencil cell of candidate k: the last s < 27 with s_first[s] <= k
         int sc = 0;
 #pragma unroll
         for (int step = 16; step > 0; step >>= 1)
           if (sc + step < 27 && s_first[sc + step] <= k) sc += step;
         const int j = w.cell_atoms[s_start[sc] + k - s_first[sc]];
-        c_pos[k] = w.pos[j];
+        const float4 pj = w.pos[j];
+        c_pos[k] = pj;
+        if (mode == FENNOL_PBC_MINIMUM_IMAGE) c_posw[k] = wrapped(pj, c, r);
         c_j[k] = j;
         c_at[k] = w.at[j];
         c_sc[k] = (unsigned char)sc;
       }
       __syncthreads();
-      for (int a = warp; a < na; a += kBuildWarps) {
+      int* q = s_queue[warp];
+      for (int a = warp; a < na; a += kCellWarps) {
         const int i = w.cell_atoms[a0 + a];
         const float4 pi = w.pos[i];
         const unsigned ati = w.at[i];
         const size_t base = (size_t)i * cap;
         int count = 0;
-        for (int k0 = 0; k0 < total; k0 += 32) {
-          const int k = k0 + lane;
-          bool keep = false;
-          int j = -1;
-          unsigned sh = 0;
-          if (k < total) {
-            j = c_j[k];
-            if (j != i) {
-              const int swrap = s_wrap[c_sc[k]];
-              keep = pair_test(mode, pi, c_pos[k], ati, c_at[k], (swrap & 3) - 1, ((swrap >> 2) & 3) - 1,
-                               ((swrap >> 4) & 3) - 1, c, r, rc2, sh);
+        if (mode == FENNOL_PBC_MINIMUM_IMAGE) {
+          // A candidate within the cutoff in the reference's minimum image lies
+          // in an adjacent cell, so that image is the box-wrapped positions
+          // plus the stencil cell's wrap: a cheap distance in that image (any
+          // rounding; 0.05 A of margin) rejects the far candidates, and the
+          // survivors, queued in candidate order, take the exact test 32 at a
+          // time.  The rows are those of the exact test alone.
+          const float4 piw = wrapped(pi, c, r);
+          auto exact_round = [&](int nq) {
+            const int kk = lane < nq ? q[lane] : -1;
+            bool keep = false;
+            int j = -1;
+            unsigned sh = 0;
+            if (kk >= 0) {
+              j = c_j[kk];
+              keep = pair_test(mode, pi, c_pos[kk], ati, c_at[kk], 0, 0, 0, c, r, rc2, sh);
+            }
+            row_append(keep, j, sh, nbr_j, nbr_shift, base, cap, count, lane);
+          };
+          int nq = 0;
+          for (int k0 = 0; k0 < total; k0 += 32) {
+            const int k = k0 + lane;
+            bool pass = false;
+            if (k < total && c_j[k] != i) {
+              const float4 pj = c_posw[k], sv4 = s_shift[c_sc[k]];
+              const float vx = (pj.x - piw.x) + sv4.x, vy = (pj.y - piw.y) + sv4.y, vz = (pj.z - piw.z) + sv4.z;
+              pass = vx * vx + vy * vy + vz * vz < rc2_pre;
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, pass);
+            if (pass) q[nq + __popc(m & lt)] = k;
+            nq += __popc(m);
+            __syncwarp();
+            if (nq >= 32) {
+              exact_round(32);
+              const int rest = lane < nq - 32 ? q[32 + lane] : 0;
+              __syncwarp();
+              if (lane < nq - 32) q[lane] = rest;
+              nq -= 32;
+              __syncwarp();
             }
           }
-          row_append(keep, j, sh, nbr_j, nbr_shift, base, cap, count, lane);
+          if (nq > 0) exact_round(nq);
+        } else {
+          for (int k0 = 0; k0 < total; k0 += 32) {
+            const int k = k0 + lane;
+            bool keep = false;
+            int j = -1;
+            unsigned sh = 0;
+            if (k < total) {
+              j = c_j[k];
+              if (j != i) {
+                const int swrap = s_wrap[c_sc[k]];
+                keep = pair_test(mode, pi, c_pos[k], ati, c_at[k], (swrap & 3) - 1, ((swrap >> 2) & 3) - 1,
+                                 ((swrap >> 4) & 3) - 1, c, r, rc2, sh);
+              }
+            }
+            row_append(keep, j, sh, nbr_j, nbr_shift, base, cap, count, lane);
+          }
         }
         row_finish(i, count, cap, nbr_count, status, lane);
+        __syncwarp();  // the queue is reused by the warp's next atom
       }
     } else {
-      for (int a = warp; a < na; a += kBuildWarps)
+      for (int a = warp; a < na; a += kCellWarps)
         cell_row(w.cell_atoms[a0 + a], atom_sys, sv, w, rc2, cap, nbr_j, nbr_shift, nbr_count, status, lane);
     }
     __syncthreads();  // the stencil tables and candidates are reused by the next cell
@@ -670,7 +741,7 @@ extern "C" int fennol_graph_build(const float* coords, int natoms, const int* at
   int gw = std::min((natoms + kBuildWarps - 1) / kBuildWarps, 148 * 16);
   if (ncells_total > 0) {
     const int gc = std::min(ncells_total, 148 * 16);
-    FNL_LAUNCH_PDL(k_build_cells_staged, gc, kBuildWarps * 32, 0, st, ncells_total, atom_sys, sv, w, rc2, capacity,
+    FNL_LAUNCH_PDL(k_build_cells_staged, gc, kCellWarps * 32, 0, st, ncells_total, atom_sys, sv, w, rc2, capacity,
                    nbr_j, nbr_shift, nbr_count, status, enable_flag);
     FNL_CHECK_LAUNCH();
   }
