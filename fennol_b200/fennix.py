@@ -150,8 +150,30 @@ def _filter_rows(layout: BatchLayout, coords: torch.Tensor, parent: NeighborRows
     return rows
 
 
-def _overflow(status: torch.Tensor, word: int) -> torch.Tensor:
-    return status[word] != 0
+class OverflowFlag:
+    """A graph layer's ``overflow`` flag (the reference's boolean array): true
+    when any of the given device status words is set.  Reading it (``bool``,
+    ``item``) copies those words to the host; nothing is launched or read
+    until then, so calls that check every status word at once never do."""
+
+    __slots__ = ("status", "words")
+
+    def __init__(self, status: torch.Tensor, words: Tuple[int, ...]):
+        self.status, self.words = status, tuple(words)
+
+    def item(self) -> bool:
+        host = self.status.cpu()
+        return any(int(host[w]) != 0 for w in self.words)
+
+    def __bool__(self) -> bool:
+        return self.item()
+
+    def __repr__(self) -> str:
+        return f"OverflowFlag({self.item()})"
+
+
+def _overflow(status: torch.Tensor, *words: int) -> OverflowFlag:
+    return OverflowFlag(status, words)
 
 
 @register_preprocessing
@@ -261,8 +283,7 @@ class GraphGenerator:
             graph["rows_skin"] = rows
             graph["rows"] = _filter_rows(layout, coords, rows, self.cutoff,
                                          int(state["max_neigh_skin"]), status)
-            graph["overflow"] = _overflow(status, _lib.ST_NBR_OVERFLOW) | _overflow(
-                status, _lib.ST_FILTER_OVERFLOW)
+            graph["overflow"] = _overflow(status, _lib.ST_NBR_OVERFLOW, _lib.ST_FILTER_OVERFLOW)
         else:
             graph["rows"] = rows
             graph["overflow"] = _overflow(status, _lib.ST_NBR_OVERFLOW)
@@ -521,8 +542,7 @@ def _species_members(inputs, species: np.ndarray) -> Dict[int, np.ndarray]:
 def _check_reallocate(layer, state, inputs, parent_overflow, own_overflow):
     """The reference's protocol (``preprocessing.py:357-367``): rerun the host
     build with a margin when this layer or a parent overflowed."""
-    if isinstance(own_overflow, torch.Tensor):
-        own_overflow = bool(own_overflow.item())
+    own_overflow = bool(own_overflow)
     if not (parent_overflow or own_overflow):
         return state, {}, inputs, False
     state, inputs, state_up = layer(state, inputs, return_state_update=True,
