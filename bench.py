@@ -783,7 +783,7 @@ def main():
     del eng, pot
     torch.cuda.empty_cache()
     # end-to-end FeNNol-API calls on every rank; the job rate uses the slowest rank
-    e2e_res = e2e(precision, box, w["n_models"], device, max(5, args.steps // 4), 2)
+    e2e_res = e2e(precision, box, w["n_models"], device, max(5, args.steps // 4), max(3, args.warmup))
     if world > 1:
         from fennol_b200.replicas import max_over_ranks
         ms_e2e = max_over_ranks(e2e_res["ms_per_step"], device)

@@ -697,6 +697,18 @@ class PreprocessingChain:
         return props
 
 
+def _status_tensors(prepared: Dict[str, Any]) -> list:
+    """The distinct device status words of the graph layers in a processed
+    inputs dictionary."""
+    pending, seen = [], set()
+    for val in prepared.values():
+        st = val.get("status") if isinstance(val, dict) else None
+        if isinstance(st, torch.Tensor) and id(st) not in seen:
+            seen.add(id(st))
+            pending.append(st)
+    return pending
+
+
 def _scaled(x: torch.Tensor, fac: float) -> torch.Tensor:
     """``x * fac`` as a new tensor; ``x`` itself (already a copy owned by the
     caller) when the factor is 1."""
@@ -917,6 +929,11 @@ class FENNIX:
         self.variables = variables
         self._pot_cache: Dict[int, Tuple[Any, ANIPotential]] = {}
         self._ws_cache = None
+        # sized calls replay a CUDA graph of the whole call (False: launch
+        # kernel by kernel, same results)
+        self.use_cuda_graphs = True
+        self._graphs: Dict[tuple, dict] = {}
+        self._graph_warm: Dict[tuple, Any] = {}
         if example_data is not None:
             self.preprocess(**example_data)
 
@@ -942,6 +959,9 @@ class FENNIX:
 
     def _workspace(self, pot: ANIPotential, layout: BatchLayout) -> Workspace:
         if self._ws_cache is None or self._ws_cache[0] is not layout or self._ws_cache[1] is not pot:
+            # captured calls use the workspace they were captured with
+            self._graphs.clear()
+            self._graph_warm.clear()
             self._ws_cache = (layout, pot, Workspace(pot, layout))
         return self._ws_cache[2]
 
@@ -994,15 +1014,9 @@ class FENNIX:
             return self.preprocess(use_gpu=gpu_preprocessing, **inputs), None
         chain = self.preprocessing
         out = chain.process(self.preproc_state, chain.check_input(inputs))
-        pending, seen = [], set()
-        for key, val in out.items():
-            if key.endswith("_overflow") and val is True:
-                return self.preprocess(use_gpu=gpu_preprocessing, **inputs), None
-            st = val.get("status") if isinstance(val, dict) else None
-            if isinstance(st, torch.Tensor) and id(st) not in seen:
-                seen.add(id(st))
-                pending.append(st)
-        return out, pending
+        if any(key.endswith("_overflow") and val is True for key, val in out.items()):
+            return self.preprocess(use_gpu=gpu_preprocessing, **inputs), None
+        return out, _status_tensors(out)
 
     def _status_host(self, rows: int) -> torch.Tensor:
         buf = getattr(self, "_status_pinned", None)
@@ -1016,15 +1030,84 @@ class FENNIX:
         capacities reruns the call through the growing preprocessing path."""
         if variables is None:
             variables = self.variables
-        prepared, pending = self._prepare(gpu_preprocessing, inputs)
-        out = self._evaluate(variables, prepared, pending=pending, **want)
+        if self.use_cuda_graphs and self._sized and self.device.type == "cuda":
+            out = self._run_graph(variables, inputs, want)
+        else:
+            prepared, pending = self._prepare(gpu_preprocessing, inputs)
+            out = self._evaluate(variables, prepared, pending=pending, **want)
         if out is None:
+            self._graphs.clear()
             prepared = self.preprocess(use_gpu=gpu_preprocessing, **inputs)
             out = self._evaluate(variables, prepared, **want)
         return out
 
+    def _run_graph(self, variables, inputs, want):
+        """A sized call replayed from a CUDA graph: the graph layers, the
+        evaluation, the output copies and the status copies, captured once per
+        batch layout, capacities, weights and outputs asked for (the last few
+        are kept).  Per call the host checks the inputs, copies the
+        coordinates in, replays, copies the outputs out and reads the status
+        words once.  Returns None when the call must take the eager path (a
+        host-side overflow, or a graph capacity that overflowed)."""
+        chain = self.preprocessing
+        inp = chain.check_input(inputs)
+        layout = inp["_layout"]
+        pot = self._potential(variables)
+        caps = tuple(tuple(sorted((k, v) for k, v in st.items() if isinstance(v, (int, float))))
+                     for st in self.preproc_state["layers_state"])
+        key = (id(layout), id(pot), caps, tuple(sorted(want.items())), self.energy_terms is None)
+        entry = self._graphs.get(key)
+        if entry is not None and (entry["layout"] is not layout or entry["pot"] is not pot):
+            entry = None
+        if entry is None and self._graph_warm.get(key) is not layout:
+            # the first call of a kind runs kernel by kernel: it creates the
+            # layout's cell plans and buffers that a capture must find ready
+            self._graph_warm[key] = layout
+            prepared = chain.process(self.preproc_state, inp)
+            if any(k.endswith("_overflow") and v is True for k, v in prepared.items()):
+                return None
+            return self._evaluate(variables, prepared, pending=_status_tensors(prepared), **want)
+        if entry is None:
+            coords = inp["_coords"].clone()
+            staged = {**inp, "_coords": coords}
+            # everything the capture needs is created before it starts
+            self._workspace(pot, layout)
+            self._status_host(2 + sum(1 for layer in chain.layers if hasattr(layer, "graph_key")))
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                prepared = chain.process(self.preproc_state, staged)
+                host_overflow = any(k.endswith("_overflow") and v is True for k, v in prepared.items())
+                pending = _status_tensors(prepared)
+                launched = self._launch(variables, prepared, pending=pending, **want)
+            if host_overflow:
+                return None
+            entry = {"graph": g, "coords": coords, "launched": launched, "layout": layout, "pot": pot}
+            while len(self._graphs) >= 4:
+                self._graphs.pop(next(iter(self._graphs)))
+            self._graphs[key] = entry
+        else:
+            entry["coords"].copy_(inp["_coords"], non_blocking=True)
+        entry["graph"].replay()
+        out, nwords, host, ws = entry["launched"]
+        # fresh output tensors for the caller: the graph's own are rewritten by
+        # the next replay
+        user = dict(out)
+        for k in (self.net_module.out_key, "total_energy", "forces", "virial_tensor",
+                  self.aev_module.embedding_key):
+            if isinstance(user.get(k), torch.Tensor):
+                user[k] = user[k].clone()
+        user.update({k: v for k, v in inp.items() if not k.startswith("_")})  # this call's inputs
+        return self._finish(user, nwords, host, ws)
+
     def _evaluate(self, variables, inputs, want_forces: bool, want_embedding: bool = False,
                   want_virial: bool = False, pending=None):
+        launched = self._launch(variables, inputs, want_forces, want_embedding, want_virial, pending)
+        return self._finish(*launched)
+
+    def _launch(self, variables, inputs, want_forces: bool, want_embedding: bool = False,
+                want_virial: bool = False, pending=None):
+        """Enqueue one evaluation: the kernels, the output copies and the copy
+        of every status word to pinned host memory (nothing waits)."""
         pot = self._potential(variables)
         layout: BatchLayout = inputs["_layout"]
         ws = self._workspace(pot, layout)
@@ -1067,10 +1150,16 @@ class FENNIX:
             mlp_err.copy_(ws.mlp_ws[:4].view(torch.int32), non_blocking=True)
         else:
             mlp_err.zero_()
+        return out, len(words), host, ws
+
+    def _finish(self, out, nwords: int, host: torch.Tensor, ws: Workspace):
+        """Wait for a launched evaluation and check its status words: None
+        when a graph capacity overflowed (the call must rerun), the outputs
+        otherwise."""
         torch.cuda.current_stream(self.device).synchronize()
-        host_words = host[:len(words) + 1].numpy().copy()
-        status, graph_words = host_words[0], host_words[1:len(words)]
-        if int(host_words[len(words), 0]):
+        host_words = host[:nwords + 1].numpy().copy()
+        status, graph_words = host_words[0], host_words[1:nwords]
+        if int(host_words[nwords, 0]):
             ws.mlp_ws[:4].view(torch.int32).zero_()
             raise _lib.KernelTimeout("species MLP: a bounded wait inside the tensor-core kernel ran out")
         if graph_words.size and (graph_words[:, _lib.ST_NBR_OVERFLOW].any()
