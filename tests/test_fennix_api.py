@@ -177,3 +177,21 @@ def test_activation_and_units():
     m = FENNIX(5.2, ani_modules(), ani_preprocessing(), energy_terms=["energy"],
                energy_unit="kcalpermol")
     assert m._unit_factor("Ha") == pytest.approx(1 / 627.5096080305927)
+
+
+def test_overflow_flag_reads_its_words_when_tested():
+    """A graph layer's overflow entry: false until one of its status words is
+    set, read from the (here host) status tensor only when tested."""
+    import torch
+
+    from fennol_b200 import _lib
+    from fennol_b200.fennix import OverflowFlag
+
+    status = torch.zeros(_lib.STATUS_WORDS, dtype=torch.int32)
+    flag = OverflowFlag(status, (_lib.ST_NBR_OVERFLOW, _lib.ST_FILTER_OVERFLOW))
+    assert not flag and flag.item() is False
+    status[_lib.ST_FILTER_OVERFLOW] = 1
+    assert flag and "True" in repr(flag)
+    status.zero_()
+    status[_lib.ST_NBR_MAXCOUNT] = 40  # other words do not count
+    assert not flag
