@@ -306,8 +306,8 @@ PRODUCTS = {"bf16": (1, 1), "bf16x2": (2, 2), "bf16x3": (3, 3), "f16x3x1": (3, 1
 
 
 def mlp_work(pot, species, precision):
-    """FLOPs per atom and model: the dense count of SURVEY-style accounting
-    (1008 inputs), the count on the AEV columns that can be non-zero for
+    """FLOPs per atom and model: the dense count over all 1008 AEV inputs
+    (2 FLOPs per multiply-add of every layer), the count on the AEV columns that can be non-zero for
     these species, and the MMA work the fused kernel issues (padded widths,
     active 64-column input chunks, split products)."""
     cols = present_aev_columns(species, pot.aev_cfg)
