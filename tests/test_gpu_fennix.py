@@ -154,6 +154,20 @@ def test_graph_replay_equals_eager_calls(cuda_device, kind):
     assert len(graph._graphs) == 1
     for e, f_copy, f in kept:
         assert torch.equal(f, f_copy)
+    # the other entry points replay graphs of their own
+    args = dict(species=sp, coordinates=xyz0.astype(np.float32), natoms=nat, **extra)
+    for _ in range(3):
+        t1, _ = graph.total_energy(**args)
+        emb1 = graph(**args)["embedding"]
+        v1 = graph.energy_and_forces_and_virial(**args)
+    t2, _ = eager.total_energy(**args)
+    emb2 = eager(**args)["embedding"]
+    v2 = eager.energy_and_forces_and_virial(**args)
+    np.testing.assert_array_equal(t1.cpu().numpy(), t2.cpu().numpy())
+    np.testing.assert_array_equal(emb1.cpu().numpy(), emb2.cpu().numpy())
+    np.testing.assert_array_equal(v1[0].cpu().numpy(), v2[0].cpu().numpy())
+    np.testing.assert_allclose(v1[2].cpu().numpy(), v2[2].cpu().numpy(), rtol=1e-5, atol=1e-6)
+    assert len(graph._graphs) == 4
 
 
 def test_skin_update_matches_fresh_build(cuda_device):
