@@ -130,8 +130,7 @@ class _EFLane:
             h_x = torch.from_numpy(xyz).pin_memory()
             coords = h_x.to(e.device, non_blocking=True)
             cap = max(b.layout.estimate_capacity(pot.aev_cfg.radial_cutoff), self.cap_hint)
-            # staged: the adjoint reuses each centre's neighbourhood the forward staged
-            g = GraphBuffers(b.layout, pot.aev_cfg.radial_cutoff, 0.0, cap, cap, stage=True)
+            g = GraphBuffers(b.layout, pot.aev_cfg.radial_cutoff, 0.0, cap, cap)
             ws = Workspace(pot, b.layout)
             st = self.stream.cuda_stream
             self._evaluate(b, coords, g, ws, st)
@@ -460,8 +459,7 @@ class ServingEngine:
         d0 = pot.mlp.dims[0]
         act = 2 * 2 if pot.precision != _lib.MLP_FP32 else 4
         # AEV rows (hi+lo or fp32) + dE/dAEV + neighbour rows + per-atom state
-        # + the single points' forward/adjoint staging (about 4.5 KB at 5.2 A)
-        self.bytes_per_atom = d0 * (act + 4) + 8 * 128 + 256 + 4608
+        self.bytes_per_atom = d0 * (act + 4) + 8 * 128 + 256
         self.bytes_per_atom_md = self.bytes_per_atom + 8 * 96 + 128
         self.bytes_in_flight = 0
         self.results: List[ServeResult] = []
